@@ -1,0 +1,68 @@
+/*
+ * libmsm.so: multi-scalar multiplication over BN254 G1.
+ *
+ * `msm` and `msm_precompute` keep the exact signatures of the reference's library
+ * (core/src/msm/src/msm.h:4-11, implemented in core/src/msm/src/msm.cu:9-48) so the Rust
+ * wrapper (core/src/msm.rs:136-369) can dlopen this library unchanged.  Scalars are 32-byte
+ * Montgomery-form Fr elements; points are 64-byte affine (x, y) Montgomery Fq with (0, 0) the
+ * identity; results are written as 64-byte affine points.
+ *
+ * The reference fixes the window width and the number of precomputed point tables per
+ * library build (libmsm_<curve>_<window>_<target_windows>_<debug>.so, core/src/msm.rs:100-111).
+ * Installed under such a name this library reads the same two fields from its file name;
+ * under any other name it uses one point table and chooses the window per call.
+ */
+#ifndef ZKP_MSM_H
+#define ZKP_MSM_H
+#include <cuda_runtime.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Synchronous MSM over host arrays (replaces msm.h:4-8, msm_impl.cuh:830-909).
+ * buffers == NULL: writes the device workspace bytes each card needs into buffer_sizes and
+ * returns (size-query protocol, msm.cu:20-22).  Otherwise buffers[k] is a caller-owned
+ * device buffer of that size on cards[k]; h_points holds the n_precompute host point tables
+ * of length len, h_scaler_batch[b] the len scalars of batch b, and h_result[b] receives the
+ * affine result of batch b.  batch_per_run, parts, stage_scalers and stage_points are the
+ * reference's host-streaming knobs; with the whole problem resident in HBM they are accepted
+ * and ignored.  Several cards each take a contiguous slice of the points; their partial
+ * results are added on cards[0]. */
+cudaError_t msm(void *const *buffers, unsigned long *buffer_sizes, unsigned long long len, unsigned int batch_per_run,
+                unsigned int parts, unsigned int stage_scalers, unsigned int stage_points, unsigned int num_cards,
+                const unsigned int *cards, unsigned int const *const *h_points, unsigned int batches,
+                unsigned int const *const *h_scaler_batch, unsigned int *const *h_result);
+
+/* Fills the host tables h_points[1 .. n_precompute-1] from h_points[0]: table j holds
+ * 2^(j * n_windows * window) * P (replaces msm.h:10 / msm_impl.cuh:776-828).  With one table
+ * there is nothing to do. */
+cudaError_t msm_precompute(unsigned long long len, unsigned int *const *h_points, unsigned int max_cards);
+
+/* ---- additions (no counterpart in the reference): asynchronous MSM over device memory ---- */
+
+/* Device workspace bytes for zkp_msm_device with n points, window bits `window` (0 = auto)
+ * and n_tables point tables (0 = the library's configuration). */
+unsigned long long zkp_msm_workspace_size(unsigned long long n, unsigned int window, unsigned int n_tables);
+
+/* Window width the library picks for n points when window == 0. */
+unsigned int zkp_msm_default_window(unsigned long long n);
+
+/* result_d (64-byte affine) = sum_i scalars_d[i] * points_d[i], asynchronous on `stream`.
+ * points_d holds n_tables contiguous tables of n affine points (table j = 2^(j*Wp*window) P
+ * with Wp = ceil(ceil(254/window) / n_tables)); workspace_d is caller-owned, at least
+ * zkp_msm_workspace_size(n, window, n_tables) bytes, and may be reused once the call's work
+ * on `stream` is done. */
+cudaError_t zkp_msm_device(void *workspace_d, unsigned long long workspace_bytes, const unsigned int *points_d,
+                           unsigned int n_tables, const unsigned int *scalars_d, unsigned long long n,
+                           unsigned int window, unsigned int *result_d, cudaStream_t stream);
+
+/* Builds the n_tables - 1 extra tables on the device: tables_d holds n_tables * n affine
+ * points and its first table is filled by the caller. */
+cudaError_t zkp_msm_precompute_device(unsigned int *tables_d, unsigned long long n, unsigned int window,
+                                      unsigned int n_tables, cudaStream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

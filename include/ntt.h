@@ -1,0 +1,65 @@
+/*
+ * libntt.so: NTT entry points over BN254 Fr (natural order in and out, in place).
+ *
+ * The first five symbols keep the exact signatures of the reference's libntt.so
+ * (core/src/ntt/src/ntt.h:5-16, implemented in core/src/ntt/src/ntt.cu:7-25) so the Rust
+ * wrappers (core/src/ntt.rs:97-371) can dlopen this library unchanged.  All device work is
+ * asynchronous on `stream`; the precompute helpers are synchronous and write host memory.
+ * Errors come back as cudaError_t (cudaErrorInvalidValue for malformed arguments).
+ *
+ * The zkp_* symbols are additions with the same conventions (no counterpart in the
+ * reference): fused inverse scaling, fused coset shift and a coset low-degree extension
+ * that reads a shorter coefficient vector.
+ */
+#ifndef ZKP_NTT_H
+#define ZKP_NTT_H
+#include <cuda_runtime.h>
+#include "poly_ptr.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Forward DFT of x (len 2^log_len) with the root table twiddle = [w^0 .. w^(n/2-1)] on the
+ * device (replaces ntt.h:6 / ssip_ntt.cuh:503-566).  The two thread-cap arguments are the
+ * reference's kernel tuning knobs; this implementation plans its own stages and ignores them. */
+cudaError_t ssip_ntt(PolyPtr x, const unsigned int *twiddle, unsigned int log_len, cudaStream_t stream,
+                     const unsigned int max_threads_stage1_log, const unsigned int max_threads_stage2_log);
+
+/* Host output: twiddle[i] = unit^i for i < len (replaces ntt.h:9 / precompute.cuh:9-87; the
+ * reference's Rust caller passes the table length, core/src/ntt.rs:226-233). */
+cudaError_t ssip_precompute(unsigned int *twiddle, unsigned int len, const unsigned int *unit);
+
+/* Forward DFT that derives its roots from omegas_d = [w, w^2, w^4, ...] instead of an n/2
+ * table (replaces ntt.h:12 / recompute_ntt.cuh:362-438). pq_d / pq_deg are accepted for ABI
+ * compatibility; the kernels rebuild every root they need from omegas_d. */
+cudaError_t recompute_ntt(PolyPtr x, const unsigned int *pq_d, unsigned int pq_deg, const unsigned int *omegas_d,
+                          unsigned int log_len, cudaStream_t stream, const unsigned int max_threads_stage1_log,
+                          const unsigned int max_threads_stage2_log);
+
+/* Host: pq[i] = (unit^(len >> pq_deg))^i for i < 2^(pq_deg-1) and omegas[i] = unit^(2^i) for
+ * i < 32, byte-identical to the reference (ntt.h:15 / precompute.cuh:89-113). */
+void gen_pq_omegas(unsigned int *pq, unsigned int *omegas, unsigned int pq_deg, unsigned int len, unsigned int *unit);
+
+/* x[i] *= powers[i % power_num] (replaces ntt.h:16 / distribute_powers.cuh:5-21). */
+cudaError_t distribute_powers(PolyPtr poly, const unsigned int *powers, unsigned long long power_num,
+                              cudaStream_t stream);
+
+/* ---- additions ---- */
+/* DFT with optional fused pre-shift x[i] *= shift^i (coset) and post-scale by *scale
+ * (inverse NTT's n^-1); shift_d / scale_d are device pointers to one element or NULL. */
+cudaError_t zkp_ntt_ex(PolyPtr x, const unsigned int *twiddle, unsigned int log_len, const unsigned int *shift_d,
+                       const unsigned int *scale_d, cudaStream_t stream);
+
+/* Coset low-degree extension: out (len 2^log_out) = DFT_{2^log_out}(in[i] * shift^i, zero
+ * padded), in has length 2^log_in <= 2^log_out; twiddle is the table for 2^log_out. */
+cudaError_t zkp_coset_lde(PolyPtr out, ConstPolyPtr in, const unsigned int *twiddle, unsigned int log_in,
+                          unsigned int log_out, const unsigned int *shift_d, cudaStream_t stream);
+
+/* Number of sub-transform passes + permutation passes the plan for 2^log_len uses. */
+unsigned int zkp_ntt_num_passes(unsigned int log_len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,128 @@
+"""Generated fused kernels and the fused quotient pipeline on the GPU, bit-exact vs the oracle."""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+M = 0x30644E72E131A029B85045B68181585D2833E84879B9709143E1F593F0000001
+
+
+def dev(zk, a):
+    return zk.ScalarArray.from_numpy(a)
+
+
+def scal(zk, a):
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.uint64).view(np.int32).reshape(1, 8).copy()).cuda()
+
+
+def zh_oracle(orc, k, ext):
+    g = orc.to_mont(orc.int_to_limbs(7))
+    gk = orc.pow_(g, 1 << k)
+    w = orc.root_of_unity(k + ext)
+    one = orc.one()
+    vals = [orc.sub(orc.mul(gk, orc.pow_(w, j << k)), one) for j in range(1 << ext)]
+    return orc.batch_invert(np.stack(vals))
+
+
+def quotient_oracle(orc, ea, eb, ec, z, zh, ext):
+    n = len(z)
+    zw = np.roll(z, -(1 << ext), axis=0)
+    t = orc.vec_sub(orc.vec_sub(orc.vec_mul(ea, eb), ec), orc.vec_mul(z, zw))
+    zhf = np.tile(zh, (n // len(zh), 1))
+    return orc.vec_mul(t, zhf)
+
+
+@pytest.mark.parametrize("log_n", [3, 10, 16])
+def test_quotient_kernel(zk, orc, log_n):
+    n = 1 << log_n
+    a, b, c, z = (orc.gen_fr(s, n) for s in (1, 2, 3, 4))
+    zh = orc.gen_fr(5, 8)
+    k = zk.fused.quotient_kernel()
+    out = zk.ScalarArray.zeros(n)
+    zd = dev(zk, z)
+    k([out], [dev(zk, a), dev(zk, b), dev(zk, c), zd, zk.pipeline.rotated(zd, 3), dev(zk, zh)])
+    assert np.array_equal(out.numpy_u64(), quotient_oracle(orc, a, b, c, z, zh, 3))
+
+
+def test_generic_graph_features(zk, orc):
+    """scalar inputs, neg, pow, Ss ops, a scalar output, Sp on Coef vs Lagrange."""
+    n = 1000
+    a = orc.gen_fr(6, n)
+    s = orc.gen_fr(7, 1)[0]
+    t = orc.gen_fr(8, 1)[0]
+    for coef in (False, True):
+        g = zk.fused.FusedGraph([
+            ("input", "a", "poly", "var", 0),
+            ("input", "s", "scalar", "var", 1),
+            ("input", "t", "scalar", "var", 2),
+            ("mul", "st", "s", "t"),
+            ("sp_add", "x", "st", "a"),
+            ("sp_subby", "y", "s", "x"),
+            ("neg", "ny", "y"),
+            ("pow", "p", "ny", 5),
+            ("output", 0, "p"),
+            ("output", 1, "st"),
+        ], coef=coef)
+        kern = zk.fused.FusedKernel(zk.fused.FusedOp(g))
+        out = zk.ScalarArray.zeros(n)
+        sout = torch.zeros((1, 8), dtype=torch.int32, device="cuda")
+        kern([out, sout], [dev(zk, a), scal(zk, s), scal(zk, t)])
+        st = orc.mul(s, t)
+        exp = []
+        for i in range(n):
+            if coef and i != 0:
+                x = a[i]
+                y = x
+            else:
+                x = orc.add(st, a[i])
+                y = orc.sub(x, s)
+            exp.append(orc.pow_(orc.neg(y), 5))
+        assert np.array_equal(out.numpy_u64(), np.stack(exp)), coef
+        assert np.array_equal(sout.cpu().numpy().view(np.uint64)[0], st)
+
+
+def test_fused_rotated_and_sliced_inputs(zk, orc):
+    n = 256
+    a = orc.gen_fr(9, n)
+    big = orc.gen_fr(10, 2 * n)
+    g = zk.fused.FusedGraph([("input", "a", "poly", "var", 0), ("input", "b", "poly", "var", 1),
+                             ("mul", "r", "a", "b"), ("output", 0, "r")])
+    kern = zk.fused.FusedKernel(zk.fused.FusedOp(g))
+    xa = dev(zk, a)
+    xa.rotate(17)
+    xb = dev(zk, big).set_slice_raw(2 * n - 3, n)
+    out = zk.ScalarArray.zeros(n)
+    kern([out], [xa, xb])
+    va = orc.poly_ptr_view(a, n, rotate=17)
+    vb = orc.poly_ptr_view(big, n, offset=2 * n - 3, whole_len=2 * n)
+    assert np.array_equal(out.numpy_u64(), orc.vec_mul(va, vb))
+
+
+@pytest.mark.parametrize("k", [10, 14])
+def test_quotient_pipeline_small(zk, orc, k):
+    ext = 3
+    n, N = 1 << k, 1 << (k + ext)
+    a, b, c = (orc.gen_fr(s, n) for s in (11, 12, 13))
+    z = orc.gen_fr(14, N)
+    pipe = zk.pipeline.QuotientPipeline(k, ext)
+    q = pipe.run(dev(zk, a), dev(zk, b), dev(zk, c), dev(zk, z))
+    g = orc.to_mont(orc.int_to_limbs(7))
+    ea, eb, ec = (orc.coset_ntt(orc.intt(x, k), k, k + ext, g) for x in (a, b, c))
+    zh = zh_oracle(orc, k, ext)
+    assert np.array_equal(zh.view(np.uint32).reshape(-1, 8), pipe.zh.numpy_u32())
+    assert np.array_equal(q.numpy_u64(), quotient_oracle(orc, ea, eb, ec, z, zh, ext))
+
+
+def test_quotient_pipeline_config3_full(zk, orc):
+    """k = 22, 8x extension (2^25), coset shift 7, bit-exact end to end."""
+    k, ext = 22, 3
+    n, N = 1 << k, 1 << (k + ext)
+    a, b, c = (orc.gen_fr(s, n) for s in (21, 22, 23))
+    z = orc.gen_fr(24, N)
+    pipe = zk.pipeline.QuotientPipeline(k, ext)
+    q = pipe.run(dev(zk, a), dev(zk, b), dev(zk, c), dev(zk, z))
+    got = q.numpy_u64()
+    g = orc.to_mont(orc.int_to_limbs(7))
+    ea, eb, ec = (orc.coset_ntt(orc.intt(x, k), k, k + ext, g) for x in (a, b, c))
+    assert np.array_equal(got, quotient_oracle(orc, ea, eb, ec, z, zh_oracle(orc, k, ext), ext))

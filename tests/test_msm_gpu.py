@@ -1,0 +1,105 @@
+"""MSM on the GPU, bit-exact (canonical affine) against the oracle's halo2 best_multiexp."""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("n", [1, 2, 7, 100, 1000, 4096])
+def test_msm_reference_abi_small(zk, orc, n):
+    s = orc.gen_fr(100 + n, n)
+    p = orc.gen_points(200 + n, n)
+    assert np.array_equal(zk.msm.msm_host(s, p), orc.best_multiexp(s, p))
+
+
+def test_msm_edge_cases(zk, orc):
+    n = 3000
+    s = orc.gen_fr(31, n)
+    p = orc.gen_points(32, n)
+    s[0:50] = 0                                  # zero scalars
+    p[50:60] = 0                                 # identity bases
+    p[60:70] = p[70:80]                          # repeated bases -> doubling inside a bucket
+    s[60:70] = s[70:80]
+    s[80] = orc.neg(s[81])                       # cancelling pair
+    p[80] = p[81]
+    s[90] = orc.to_mont(orc.int_to_limbs(1))     # scalar 1
+    s[91] = orc.neg(orc.to_mont(orc.int_to_limbs(1)))  # r - 1
+    assert np.array_equal(zk.msm.msm_host(s, p), orc.best_multiexp(s, p))
+
+
+def test_msm_all_equal_scalars_one_bucket(zk, orc):
+    """Every digit lands in the same bucket of each window: runs cross many chunks."""
+    n = 1 << 14
+    s = np.repeat(orc.gen_fr(41, 1), n, axis=0)
+    p = orc.gen_points(42, n)
+    assert np.array_equal(zk.msm.msm_host(s, p), orc.best_multiexp(s, p))
+
+
+def test_msm_zero_result_and_all_zero(zk, orc):
+    n = 64
+    p = orc.gen_points(43, n)
+    s = np.zeros((n, 4), dtype=np.uint64)
+    assert np.array_equal(zk.msm.msm_host(s, p), np.zeros(8, dtype=np.uint64))
+    s = orc.gen_fr(44, n)
+    s[n // 2:] = np.stack([orc.neg(x) for x in s[: n // 2]])
+    p[n // 2:] = p[: n // 2]
+    assert np.array_equal(zk.msm.msm_host(s, p), np.zeros(8, dtype=np.uint64))
+
+
+@pytest.mark.parametrize("window", [8, 11, 13, 16, 20])
+def test_msm_device_windows(zk, orc, window):
+    n = 5000
+    s = orc.gen_fr(50 + window, n)
+    p = orc.gen_points(60 + window, n)
+    bases = zk.msm.ResidentBases(p, window=window)
+    res = torch.zeros(16, dtype=torch.int32, device="cuda")
+    dev_s = torch.from_numpy(s.view(np.int32).reshape(n, 8).copy()).cuda()
+    bases.msm(dev_s, res, bases.workspace())
+    got = res.cpu().numpy().view(np.uint64)
+    assert np.array_equal(got, orc.best_multiexp(s, p))
+
+
+@pytest.mark.parametrize("window,n_tables", [(16, 2), (13, 4), (16, 16)])
+def test_msm_precomputed_tables(zk, orc, window, n_tables):
+    n = 3000
+    s = orc.gen_fr(70 + n_tables, n)
+    p = orc.gen_points(80 + n_tables, n)
+    bases = zk.msm.ResidentBases(p, window=window, n_tables=n_tables)
+    res = torch.zeros(16, dtype=torch.int32, device="cuda")
+    ws = bases.workspace()
+    for trial in range(2):  # workspace reuse
+        dev_s = torch.from_numpy(s.view(np.int32).reshape(n, 8).copy()).cuda()
+        bases.msm(dev_s, res, ws)
+        assert np.array_equal(res.cpu().numpy().view(np.uint64), orc.best_multiexp(s, p)), trial
+        s = orc.gen_fr(90 + trial, n)
+
+
+def test_msm_batches_share_points(zk, orc):
+    n = 2000
+    p = orc.gen_points(91, n)
+    batches = [orc.gen_fr(92 + b, n) for b in range(4)]
+    res = zk.msm.msm_host_batches([b.view(np.uint32).reshape(n, 8) for b in batches],
+                                  [p.view(np.uint32).reshape(n, 16)])
+    for b, r in zip(batches, res):
+        assert np.array_equal(r.view(np.uint64), orc.best_multiexp(b, p))
+
+
+def test_msm_size_query(zk):
+    sizes = zk.msm.MSM().get_buffer_size(1 << 20)
+    assert len(sizes) == 1 and sizes[0] > (1 << 20) * 96
+
+
+def test_config2_msm_2_20(zk, orc):
+    """n = 2^20, scalars seed 1, points k_i * G with k_i from seed 2."""
+    n = 1 << 20
+    s = orc.gen_fr(1, n)
+    p = orc.gen_points(2, n)
+    assert np.array_equal(zk.msm.msm_host(s, p), orc.best_multiexp(s, p))
+
+
+def test_msm_2_22_metric_size(zk, orc):
+    n = 1 << 22
+    s = orc.gen_fr(1, n)
+    p = orc.gen_points(2, n)
+    assert np.array_equal(zk.msm.msm_host(s, p), orc.best_multiexp(s, p))

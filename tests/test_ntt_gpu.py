@@ -1,0 +1,156 @@
+"""NTT family on the GPU through the C ABI, bit-exact against the CPU oracle."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def to_dev(zk, a):
+    return zk.ScalarArray.from_numpy(a)
+
+
+@pytest.mark.parametrize("log_n", list(range(1, 17)) + [18, 20])
+def test_ssip_ntt_matches_best_fft(zk, orc, log_n):
+    n = 1 << log_n
+    a = orc.gen_fr(0 if log_n == 16 else 40 + log_n, n)
+    x = to_dev(zk, a)
+    zk.ntt.ssip_ntt(x, zk.ntt.twiddle_table(log_n))
+    expect = orc.best_fft(a, orc.root_of_unity(log_n), log_n)
+    assert np.array_equal(x.numpy_u64(), expect)
+
+
+@pytest.mark.parametrize("log_n", [1, 5, 12, 13, 16, 25])
+def test_intt_roundtrip(zk, orc, log_n):
+    n = 1 << log_n
+    a = orc.gen_fr(7, n)
+    x = to_dev(zk, a)
+    zk.ntt.ntt(x)
+    zk.ntt.intt(x)
+    assert np.array_equal(x.numpy_u64(), a)
+
+
+def test_intt_matches_oracle(zk, orc):
+    log_n = 14
+    a = orc.gen_fr(70, 1 << log_n)
+    x = to_dev(zk, a)
+    zk.ntt.intt(x)
+    assert np.array_equal(x.numpy_u64(), orc.intt(a, log_n))
+
+
+def test_config1_roundtrip_2_16(zk, orc):
+    """NTT 2^16 of seed-0 data, bit-exact vs best_fft, then INTT round trip."""
+    a = orc.gen_fr(0, 1 << 16)
+    x = to_dev(zk, a)
+    zk.ntt.ntt(x)
+    assert np.array_equal(x.numpy_u64(), orc.ntt(a, 16))
+    zk.ntt.intt(x)
+    assert np.array_equal(x.numpy_u64(), a)
+
+
+def test_ntt_2_24_properties(zk, orc):
+    """Full metric size: round trip and linearity NTT(a + b) = NTT(a) + NTT(b) at 2^24."""
+    import torch
+    log_n = 24
+    n = 1 << log_n
+    a = orc.gen_fr(1, n)
+    b = orc.gen_fr(2, n)
+    xa, xb = to_dev(zk, a), to_dev(zk, b)
+    xs = to_dev(zk, orc.vec_add(a, b))
+    for x in (xa, xb, xs):
+        zk.ntt.ntt(x)
+    # spot-check entries against direct evaluation at w^k
+    w = orc.root_of_unity(log_n)
+    got = xa.values.cpu().numpy().view(np.uint64).reshape(-1, 4)
+    for k in (0, 1, 12345, n - 1):
+        assert np.array_equal(got[k], orc.eval_poly(a, orc.pow_(w, k))), k
+    sa = orc.vec_add(got, xb.values.cpu().numpy().view(np.uint64).reshape(-1, 4))
+    assert np.array_equal(sa, xs.values.cpu().numpy().view(np.uint64).reshape(-1, 4))
+    zk.ntt.intt(xa)
+    assert np.array_equal(xa.values.cpu().numpy().view(np.uint64).reshape(-1, 4), a)
+    del torch
+
+
+@pytest.mark.parametrize("log_n", [3, 11, 15])
+def test_rotated_and_sliced_views(zk, orc, log_n):
+    n = 1 << log_n
+    base = orc.gen_fr(5, n)
+    # rotated whole array
+    x = to_dev(zk, base)
+    x.rotate(3)
+    view = orc.poly_ptr_view(base, n, rotate=3)
+    zk.ntt.ssip_ntt(x, zk.ntt.twiddle_table(log_n))
+    assert np.array_equal(x.numpy_u64(), orc.ntt(view, log_n))
+    # slice of a larger buffer that wraps around its end
+    big = orc.gen_fr(6, 2 * n)
+    xb = to_dev(zk, big)
+    s = xb.set_slice_raw(2 * n - 5, n)
+    view = orc.poly_ptr_view(big, n, offset=2 * n - 5, whole_len=2 * n)
+    zk.ntt.ssip_ntt(s, zk.ntt.twiddle_table(log_n))
+    assert np.array_equal(s.numpy_u64(), orc.ntt(view, log_n))
+    # the part of the buffer outside the slice is untouched
+    after = xb.values.cpu().numpy().view(np.uint64).reshape(-1, 4)
+    untouched = [i for i in range(2 * n) if not (i >= 2 * n - 5 or i < n - 5)]
+    assert np.array_equal(after[untouched], big[untouched])
+
+
+@pytest.mark.parametrize("log_n", [4, 12, 17])
+def test_recompute_ntt(zk, orc, log_n):
+    n = 1 << log_n
+    a = orc.gen_fr(9, n)
+    w = zk.field.mont_words(zk.field.root_of_unity(log_n))
+    pq_len = zk.ntt.get_pq_len(log_n)
+    pq, omegas = zk.ntt.gen_pq_omegas(pq_len, n, w)
+    x = to_dev(zk, a)
+    zk.ntt.recompute_ntt(x, zk.ScalarArray.from_numpy(pq), zk.ScalarArray.from_numpy(omegas))
+    assert np.array_equal(x.numpy_u64(), orc.ntt(a, log_n))
+
+
+def test_precompute_tables(zk, orc):
+    w = orc.root_of_unity(12)
+    tab = zk.ntt.ssip_precompute(2048, w.view(np.uint32))
+    assert np.array_equal(tab.view(np.uint64).reshape(-1, 4), orc.twiddles(w, 2048))
+    assert np.array_equal(zk.ntt.ssip_precompute(1, w.view(np.uint32)).view(np.uint64).reshape(-1, 4)[0],
+                          orc.one())
+
+
+def test_distribute_powers(zk, orc):
+    a = orc.gen_fr(10, 1000)
+    for pn in (1, 7, 64, 1000, 2000):
+        p = orc.gen_fr(11, pn)
+        x = to_dev(zk, a)
+        zk.ntt.distribute_powers(x, zk.ScalarArray.from_numpy(p))
+        assert np.array_equal(x.numpy_u64(), orc.distribute_powers(a, p)), pn
+
+
+@pytest.mark.parametrize("log_in,log_out", [(2, 5), (10, 13), (13, 16), (16, 19)])
+def test_coset_lde(zk, orc, log_in, log_out):
+    coef = orc.gen_fr(12, 1 << log_in)
+    g = orc.to_mont(orc.int_to_limbs(7))
+    out = zk.ScalarArray.zeros(1 << log_out)
+    zk.ntt.coset_ntt(out, to_dev(zk, coef))
+    assert np.array_equal(out.numpy_u64(), orc.coset_ntt(coef, log_in, log_out, g))
+
+
+def test_ntt_ex_shift_and_scale(zk, orc):
+    log_n = 14
+    a = orc.gen_fr(13, 1 << log_n)
+    g = orc.to_mont(orc.int_to_limbs(5))
+    x = to_dev(zk, a)
+    zk.ntt.ntt_ex(x, zk.ntt.twiddle_table(log_n), shift=zk.ntt.scalar_const(5), scale=zk.ntt.scalar_const(3))
+    expect = orc.coset_ntt(a, log_n, log_n, g)
+    three = orc.to_mont(orc.int_to_limbs(3))
+    expect = np.stack([orc.mul(e, three) for e in expect])
+    assert np.array_equal(x.numpy_u64(), expect)
+
+
+def test_invalid_arguments_return_error(zk):
+    x = zk.ScalarArray.zeros(16)
+    bad = x.poly_ptr()
+    bad.len = 15
+    lib = zk.native.load("libntt.so")
+    tw = zk.ntt.twiddle_table(4)
+    assert lib.ssip_ntt(bad, tw.values.data_ptr(), 4, None, 8, 8) == 1  # cudaErrorInvalidValue
+    bad = x.poly_ptr()
+    bad.rotate = 3
+    bad.offset = 2
+    assert lib.ssip_ntt(bad, tw.values.data_ptr(), 4, None, 8, 8) == 1

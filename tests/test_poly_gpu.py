@@ -1,0 +1,128 @@
+"""Poly library on the GPU through the C ABI, bit-exact against the oracle / big integers."""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+M = 0x30644E72E131A029B85045B68181585D2833E84879B9709143E1F593F0000001
+R = 1 << 256
+
+
+def dev(zk, a):
+    return zk.ScalarArray.from_numpy(a)
+
+
+def scal(zk, a):
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.uint64).view(np.int32).reshape(1, 8).copy()).cuda()
+
+
+def ints(orc, a):
+    """canonical integers of Montgomery-form limbs"""
+    return [orc.limbs_to_int(x) * pow(R, -1, M) % M for x in a]
+
+
+@pytest.mark.parametrize("la,lb", [(1000, 1000), (1000, 300), (300, 1000)])
+def test_binary_ops_unequal_lengths(zk, orc, la, lb):
+    a, b = orc.gen_fr(1, la), orc.gen_fr(2, lb)
+    up, lo = max(la, lb), min(la, lb)
+    for name, fn in (("add", zk.poly.poly_add), ("sub", zk.poly.poly_sub), ("mul", zk.poly.poly_mul)):
+        r = zk.ScalarArray.zeros(up)
+        fn(r, dev(zk, a), dev(zk, b))
+        got = r.numpy_u64()
+        head = {"add": orc.vec_add, "sub": orc.vec_sub, "mul": orc.vec_mul}[name](a[:lo], b[:lo])
+        assert np.array_equal(got[:lo], head), name
+        longer = a if la >= lb else b
+        tail = longer[lo:]
+        if name == "sub" and la < lb:
+            tail = np.stack([orc.neg(x) for x in tail])
+        assert np.array_equal(got[lo:], tail), name
+
+
+def test_binary_ops_rotated(zk, orc):
+    n = 512
+    a, b = orc.gen_fr(3, n), orc.gen_fr(4, n)
+    xa, xb = dev(zk, a), dev(zk, b)
+    xa.rotate(5)
+    xb.rotate(n - 7)
+    r = zk.ScalarArray.zeros(n)
+    r.rotate(11)
+    zk.poly.poly_mul(r, xa, xb)
+    va = orc.poly_ptr_view(a, n, rotate=5)
+    vb = orc.poly_ptr_view(b, n, rotate=n - 7)
+    assert np.array_equal(r.numpy_u64(), orc.vec_mul(va, vb))
+
+
+def test_fills(zk, orc):
+    t = dev(zk, orc.gen_fr(5, 100))
+    zk.poly.poly_one_lagrange(t)
+    assert np.array_equal(t.numpy_u64(), np.repeat(orc.one()[None], 100, 0))
+    zk.poly.poly_one_coef(t)
+    got = t.numpy_u64()
+    assert np.array_equal(got[0], orc.one()) and not got[1:].any()
+    zk.poly.poly_zero(t)
+    assert not t.numpy_u64().any()
+
+
+@pytest.mark.parametrize("n", [1, 5, 64, 65, 4097, 1 << 20])
+def test_poly_eval(zk, orc, n):
+    a = orc.gen_fr(6, n)
+    x = orc.gen_fr(7, 1)[0]
+    res = torch.zeros((1, 8), dtype=torch.int32, device="cuda")
+    zk.poly.poly_eval(dev(zk, a), scal(zk, x), res)
+    assert np.array_equal(res.cpu().numpy().view(np.uint64)[0], orc.eval_poly(a, x))
+
+
+@pytest.mark.parametrize("n", [1, 63, 64, 65, 5000, 1 << 20])
+def test_batched_invert(zk, orc, n):
+    a = orc.gen_fr(8, n)
+    if n > 10:
+        a[3] = 0
+        a[n - 1] = 0
+        a[64:128 if n > 128 else n] = 0  # a whole zero chunk
+    t = dev(zk, a)
+    zk.poly.batched_invert(t)
+    assert np.array_equal(t.numpy_u64(), orc.batch_invert(a))
+
+
+@pytest.mark.parametrize("n", [1, 64, 65, 4100, 70000])
+def test_scan_mul(zk, orc, n):
+    a = orc.gen_fr(9, n)
+    t = dev(zk, a)
+    zk.poly.scan_mul(t)
+    got = ints(orc, t.numpy_u64())
+    acc, expect = 1, []
+    for v in ints(orc, a):
+        acc = acc * v % M
+        expect.append(acc)
+    assert got == expect
+
+
+@pytest.mark.parametrize("log_n", [0, 1, 4, 6, 7, 12, 16])
+def test_kate_division(zk, orc, log_n):
+    n = 1 << log_n
+    p = orc.gen_fr(10, n)
+    b = orc.gen_fr(11, 1)[0]
+    q = zk.ScalarArray.zeros(n)
+    xp = dev(zk, p)
+    xp.rotate(2 % n if n > 1 else 0)
+    zk.poly.kate_division(xp, scal(zk, b), q)
+    pv = ints(orc, orc.poly_ptr_view(p, n, rotate=2 % n if n > 1 else 0))
+    bi = ints(orc, [b])[0]
+    expect = [0] * n
+    for i in range(n - 2, -1, -1):
+        expect[i] = (pv[i + 1] + bi * expect[i + 1]) % M
+    assert ints(orc, q.numpy_u64()) == expect
+
+
+def test_scalar_inv_and_pow(zk, orc):
+    x = orc.gen_fr(12, 1)[0]
+    t = scal(zk, x)
+    zk.poly.inv_scalar(t)
+    assert np.array_equal(t.cpu().numpy().view(np.uint64)[0], orc.inv(x))
+    t = scal(zk, x)
+    zk.poly.scalar_pow(t, 12345678901)
+    assert np.array_equal(t.cpu().numpy().view(np.uint64)[0], orc.pow_(x, 12345678901))
+    z = scal(zk, np.zeros(4, dtype=np.uint64))
+    zk.poly.inv_scalar(z)
+    assert not z.cpu().numpy().any()

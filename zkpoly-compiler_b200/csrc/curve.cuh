@@ -1,0 +1,272 @@
+// BN254 G1 (y^2 = x^3 + 3 over Fq) in XYZZ and affine coordinates, device side.
+//
+// Formulas are the EFD XYZZ ones the reference uses (core/src/common/curve/src/
+// curve_xyzz.cuh:252-391): madd-2008-s, add-2008-s, dbl-2008-s-1 and mdbl-2008-s-1.  Affine
+// points are (x, y) Montgomery Fq with (0, 0) the identity (PointAffine::is_identity tests
+// y == 0); an XYZZ point is the identity when zz == 0.
+//
+// Coordinates are lazy ([0, 2q)), so every "is zero" decision reduces modulo q first.
+#pragma once
+#include "field.cuh"
+
+namespace zk {
+
+struct G1A {
+    Fq x, y;
+
+    ZK_DI static G1A load(const u32 *p) {
+        G1A r;
+        r.x = Fq::load(p);
+        r.y = Fq::load(p + 8);
+        return r;
+    }
+    ZK_DI static G1A load_nc(const u32 *p) {
+        G1A r;
+        r.x = Fq::load_nc(p);
+        r.y = Fq::load_nc(p + 8);
+        return r;
+    }
+    ZK_DI void store(u32 *p) const {
+        x.store(p);
+        y.store(p + 8);
+    }
+    ZK_DI bool is_identity() const { return y.canonical().is_zero(); }
+    ZK_DI G1A neg() const {
+        G1A r;
+        r.x = x;
+        r.y = Fq::neg(y);
+        return r;
+    }
+};
+
+struct G1X {
+    Fq x, y, zz, zzz;
+
+    ZK_DI static G1X identity() {
+        G1X r;
+        r.x = Fq::zero();
+        r.y = Fq::zero();
+        r.zz = Fq::zero();
+        r.zzz = Fq::zero();
+        return r;
+    }
+    ZK_DI static G1X from_affine(const G1A &a) {
+        if (a.is_identity()) return identity();
+        G1X r;
+        r.x = a.x;
+        r.y = a.y;
+        r.zz = Fq::one();
+        r.zzz = Fq::one();
+        return r;
+    }
+    ZK_DI bool is_identity() const { return zz.canonical().is_zero(); }
+
+    ZK_DI static G1X load(const u32 *p) {
+        G1X r;
+        r.x = Fq::load(p);
+        r.y = Fq::load(p + 8);
+        r.zz = Fq::load(p + 16);
+        r.zzz = Fq::load(p + 24);
+        return r;
+    }
+    ZK_DI void store(u32 *p) const {
+        x.store(p);
+        y.store(p + 8);
+        zz.store(p + 16);
+        zzz.store(p + 24);
+    }
+    ZK_DI G1X neg() const {
+        G1X r = *this;
+        r.y = Fq::neg(y);
+        return r;
+    }
+};
+
+// mdbl-2008-s-1: 2 * (x, y) for an affine point (curve_xyzz.cuh:229-241)
+ZK_DI G1X g1_dbl_affine(const G1A &p) {
+    Fq u = Fq::dbl(p.y);
+    Fq v = Fq::sqr(u);
+    Fq w = Fq::mul(u, v);
+    Fq s = Fq::mul(p.x, v);
+    Fq x2 = Fq::sqr(p.x);
+    Fq m = Fq::add(Fq::dbl(x2), x2);
+    G1X r;
+    r.x = Fq::sub(Fq::sub(Fq::sqr(m), s), s);
+    r.y = Fq::sub(Fq::mul(m, Fq::sub(s, r.x)), Fq::mul(w, p.y));
+    r.zz = v;
+    r.zzz = w;
+    return r;
+}
+
+// dbl-2008-s-1 (curve_xyzz.cuh:377-391)
+ZK_DI G1X g1_dbl(const G1X &p) {
+    if (p.is_identity()) return p;
+    Fq u = Fq::dbl(p.y);
+    Fq v = Fq::sqr(u);
+    Fq w = Fq::mul(u, v);
+    Fq s = Fq::mul(p.x, v);
+    Fq x2 = Fq::sqr(p.x);
+    Fq m = Fq::add(Fq::dbl(x2), x2);
+    G1X r;
+    r.x = Fq::sub(Fq::sub(Fq::sqr(m), s), s);
+    r.y = Fq::sub(Fq::mul(m, Fq::sub(s, r.x)), Fq::mul(w, p.y));
+    r.zz = Fq::mul(v, p.zz);
+    r.zzz = Fq::mul(w, p.zzz);
+    return r;
+}
+
+// madd-2008-s: XYZZ + affine (curve_xyzz.cuh:352-370)
+ZK_DI G1X g1_madd(const G1X &a, const G1A &b) {
+    if (b.is_identity()) return a;
+    if (a.is_identity()) return G1X::from_affine(b);
+    Fq u2 = Fq::mul(b.x, a.zz);
+    Fq s2 = Fq::mul(b.y, a.zzz);
+    Fq p = Fq::sub(u2, a.x);
+    Fq r = Fq::sub(s2, a.y);
+    if (p.canonical().is_zero() && r.canonical().is_zero()) return g1_dbl_affine(b);
+    Fq pp = Fq::sqr(p);
+    Fq ppp = Fq::mul(p, pp);
+    Fq q = Fq::mul(a.x, pp);
+    G1X o;
+    o.x = Fq::sub(Fq::sub(Fq::sub(Fq::sqr(r), ppp), q), q);
+    o.y = Fq::sub(Fq::mul(r, Fq::sub(q, o.x)), Fq::mul(a.y, ppp));
+    o.zz = Fq::mul(a.zz, pp);
+    o.zzz = Fq::mul(a.zzz, ppp);
+    return o;
+}
+
+// add-2008-s: XYZZ + XYZZ (curve_xyzz.cuh:325-345)
+ZK_DI G1X g1_add(const G1X &a, const G1X &b) {
+    if (a.is_identity()) return b;
+    if (b.is_identity()) return a;
+    Fq u1 = Fq::mul(a.x, b.zz);
+    Fq u2 = Fq::mul(b.x, a.zz);
+    Fq s1 = Fq::mul(a.y, b.zzz);
+    Fq s2 = Fq::mul(b.y, a.zzz);
+    Fq p = Fq::sub(u2, u1);
+    Fq r = Fq::sub(s2, s1);
+    if (p.canonical().is_zero() && r.canonical().is_zero()) return g1_dbl(a);
+    Fq pp = Fq::sqr(p);
+    Fq ppp = Fq::mul(p, pp);
+    Fq q = Fq::mul(u1, pp);
+    G1X o;
+    o.x = Fq::sub(Fq::sub(Fq::sub(Fq::sqr(r), ppp), q), q);
+    o.y = Fq::sub(Fq::mul(r, Fq::sub(q, o.x)), Fq::mul(s1, ppp));
+    o.zz = Fq::mul(Fq::mul(a.zz, b.zz), pp);
+    o.zzz = Fq::mul(Fq::mul(a.zzz, b.zzz), ppp);
+    return o;
+}
+
+// k * p by double-and-add over the bits of a 64-bit k
+ZK_DI G1X g1_mul_u64(const G1X &p, u64 k) {
+    G1X acc = G1X::identity();
+    if (k == 0) return acc;
+    int top = 63 - __clzll(k);
+    acc = p;
+    for (int i = top - 1; i >= 0; i--) {
+        acc = g1_dbl(acc);
+        if ((k >> i) & 1) acc = g1_add(acc, p);
+    }
+    return acc;
+}
+
+// ------------------------------------------------------------------ inversion for the
+// latency-critical single-thread tail: binary extended Euclid on plain integers.
+// Input a = x R mod q (Montgomery form, x != 0); returns x^-1 R mod q.
+ZK_DI void bn_rshift1(u32 *a) {
+#pragma unroll
+    for (int i = 0; i < 7; i++) a[i] = (a[i] >> 1) | (a[i + 1] << 31);
+    a[7] >>= 1;
+}
+ZK_DI bool bn_is_one(const u32 *a) {
+    u32 acc = a[0] ^ 1u;
+#pragma unroll
+    for (int i = 1; i < 8; i++) acc |= a[i];
+    return acc == 0;
+}
+ZK_DI bool bn_geq(const u32 *a, const u32 *b) {
+    for (int i = 7; i >= 0; i--) {
+        if (a[i] != b[i]) return a[i] > b[i];
+    }
+    return true;
+}
+// (x + q) / 2 or x / 2 modulo q for x < q
+template <class P>
+ZK_DI void half_mod(u32 *x) {
+    if (x[0] & 1u) {
+        u32 c;
+        x[0] = add_cc(x[0], P::m(0));
+#pragma unroll
+        for (int i = 1; i < 8; i++) x[i] = addc_cc(x[i], P::m(i));
+        c = addc(0u, 0u);
+        bn_rshift1(x);
+        x[7] |= c << 31;
+    } else {
+        bn_rshift1(x);
+    }
+}
+
+template <class P>
+ZK_DI Fp<P> inv_binary(const Fp<P> &a_mont) {
+    using F = Fp<P>;
+    F a = a_mont.canonical();
+    if (a.is_zero()) return F::zero();
+    u32 u[8], v[8], x1[8], x2[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        u[i] = a.v[i];
+        v[i] = P::m(i);
+        x1[i] = 0;
+        x2[i] = 0;
+    }
+    x1[0] = 1;
+    // invariant: x1 * a == u, x2 * a == v (mod q)
+    while (!bn_is_one(u) && !bn_is_one(v)) {
+        while ((u[0] & 1u) == 0) {
+            bn_rshift1(u);
+            half_mod<P>(x1);
+        }
+        while ((v[0] & 1u) == 0) {
+            bn_rshift1(v);
+            half_mod<P>(x2);
+        }
+        if (bn_geq(u, v)) {
+            F::sub_raw(u, u, v);
+            F t1 = F::from_words(x1), t2 = F::from_words(x2);
+            F d = F::sub_c(t1, t2);
+#pragma unroll
+            for (int i = 0; i < 8; i++) x1[i] = d.v[i];
+        } else {
+            F::sub_raw(v, v, u);
+            F t1 = F::from_words(x1), t2 = F::from_words(x2);
+            F d = F::sub_c(t2, t1);
+#pragma unroll
+            for (int i = 0; i < 8; i++) x2[i] = d.v[i];
+        }
+    }
+    F r = bn_is_one(u) ? F::from_words(x1) : F::from_words(x2);
+    // r = (xR)^-1 = x^-1 R^-1; multiply by R^3 in Montgomery to get x^-1 R
+    F r2;
+#pragma unroll
+    for (int i = 0; i < 8; i++) r2.v[i] = P::r2(i);
+    r = F::mul(r, r2);  // x^-1 R^-1 * R^2 * R^-1 = x^-1 R^0 ... times R below
+    r = F::mul(r, r2);  // x^-1 * R^2 * R^-1 = x^-1 R
+    return r.canonical();
+}
+
+// XYZZ -> affine (scaling-z, curve_xyzz.cuh:316-322); identity -> (0, 0)
+ZK_DI G1A g1_to_affine(const G1X &p) {
+    G1A r;
+    if (p.is_identity()) {
+        r.x = Fq::zero();
+        r.y = Fq::zero();
+        return r;
+    }
+    Fq a = inv_binary<FqParams>(p.zzz);
+    Fq b = Fq::sqr(Fq::mul(p.zz, a));
+    r.x = Fq::mul(p.x, b).canonical();
+    r.y = Fq::mul(p.y, a).canonical();
+    return r;
+}
+
+}  // namespace zk

@@ -1,0 +1,348 @@
+// BN254 Fr / Fq Montgomery arithmetic for sm_100a.
+//
+// Semantics follow the reference's mont::Element (core/src/common/mont/src/field.cuh:906-1204):
+// an element is 8 little-endian u32 limbs in Montgomery form (R = 2^256), and every value a
+// kernel stores is canonical (< m), so bytes match the reference and the oracle exactly.
+//
+// Inside kernels values are kept "lazy" in [0, 2m): both moduli are below 2^254, so with
+// 4m < R the CIOS product of two values below 2m is again below 2m and needs no final
+// subtraction; additions and subtractions fold back into [0, 2m) with one conditional
+// correction.  `canonical()` maps [0, 2m) to [0, m) before a store.
+//
+// The multiply is word-serial CIOS with two carry chains per row (low halves, then high
+// halves) on mad.lo.cc / madc.hi.cc; the low word of the reduction row is replaced by a
+// carry test because it is zero by construction.
+#pragma once
+#include <cstdint>
+
+namespace zk {
+
+using u32 = uint32_t;
+using u64 = uint64_t;
+
+// ------------------------------------------------------------------ PTX carry primitives
+#define ZK_DI __device__ __forceinline__
+
+ZK_DI u32 add_cc(u32 a, u32 b) { u32 r; asm volatile("add.cc.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b)); return r; }
+ZK_DI u32 addc_cc(u32 a, u32 b) { u32 r; asm volatile("addc.cc.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b)); return r; }
+ZK_DI u32 addc(u32 a, u32 b) { u32 r; asm volatile("addc.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b)); return r; }
+ZK_DI u32 sub_cc(u32 a, u32 b) { u32 r; asm volatile("sub.cc.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b)); return r; }
+ZK_DI u32 subc_cc(u32 a, u32 b) { u32 r; asm volatile("subc.cc.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b)); return r; }
+ZK_DI u32 subc(u32 a, u32 b) { u32 r; asm volatile("subc.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b)); return r; }
+ZK_DI u32 mad_lo_cc(u32 a, u32 b, u32 c) { u32 r; asm volatile("mad.lo.cc.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(c)); return r; }
+ZK_DI u32 madc_lo_cc(u32 a, u32 b, u32 c) { u32 r; asm volatile("madc.lo.cc.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(c)); return r; }
+ZK_DI u32 mad_hi_cc(u32 a, u32 b, u32 c) { u32 r; asm volatile("mad.hi.cc.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(c)); return r; }
+ZK_DI u32 madc_hi_cc(u32 a, u32 b, u32 c) { u32 r; asm volatile("madc.hi.cc.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(c)); return r; }
+ZK_DI u32 madc_hi(u32 a, u32 b, u32 c) { u32 r; asm volatile("madc.hi.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(c)); return r; }
+
+// ------------------------------------------------------------------ field parameters
+// moduli from core/src/common/mont/src/bn254_fr.cuh:18-26 and bn254_fq.cuh:10-18
+struct FrParams {
+    ZK_DI static constexpr u32 m(int i) {
+        constexpr u32 t[8] = {0xf0000001u, 0x43e1f593u, 0x79b97091u, 0x2833e848u,
+                                 0x8181585du, 0xb85045b6u, 0xe131a029u, 0x30644e72u};
+        return t[i];
+    }
+    ZK_DI static constexpr u32 m2(int i) {
+        constexpr u32 t[8] = {0xe0000002u, 0x87c3eb27u, 0xf372e122u, 0x5067d090u,
+                                  0x0302b0bau, 0x70a08b6du, 0xc2634053u, 0x60c89ce5u};
+        return t[i];
+    }
+    ZK_DI static constexpr u32 r1(int i) {
+        constexpr u32 t[8] = {0x4ffffffbu, 0xac96341cu, 0x9f60cd29u, 0x36fc7695u,
+                                  0x7879462eu, 0x666ea36fu, 0x9a07df2fu, 0x0e0a77c1u};
+        return t[i];
+    }
+    ZK_DI static constexpr u32 r2(int i) {
+        constexpr u32 t[8] = {0xae216da7u, 0x1bb8e645u, 0xe35c59e3u, 0x53fe3ab1u,
+                                  0x53bb8085u, 0x8c49833du, 0x7f4e44a5u, 0x0216d0b1u};
+        return t[i];
+    }
+    static constexpr u32 MPRIME = 4026531839u;  // -m^-1 mod 2^32
+};
+
+struct FqParams {
+    ZK_DI static constexpr u32 m(int i) {
+        constexpr u32 t[8] = {0xd87cfd47u, 0x3c208c16u, 0x6871ca8du, 0x97816a91u,
+                                 0x8181585du, 0xb85045b6u, 0xe131a029u, 0x30644e72u};
+        return t[i];
+    }
+    ZK_DI static constexpr u32 m2(int i) {
+        constexpr u32 t[8] = {0xb0f9fa8eu, 0x7841182du, 0xd0e3951au, 0x2f02d522u,
+                                  0x0302b0bbu, 0x70a08b6du, 0xc2634053u, 0x60c89ce5u};
+        return t[i];
+    }
+    ZK_DI static constexpr u32 r1(int i) {
+        constexpr u32 t[8] = {0xc58f0d9du, 0xd35d438du, 0xf5c70b3du, 0x0a78eb28u,
+                                  0x7879462cu, 0x666ea36fu, 0x9a07df2fu, 0x0e0a77c1u};
+        return t[i];
+    }
+    ZK_DI static constexpr u32 r2(int i) {
+        constexpr u32 t[8] = {0x538afa89u, 0xf32cfc5bu, 0xd44501fbu, 0xb5e71911u,
+                                  0x0a417ff6u, 0x47ab1effu, 0xcab8351fu, 0x06d89f71u};
+        return t[i];
+    }
+    static constexpr u32 MPRIME = 3834012553u;
+};
+
+template <class P>
+struct Fp {
+    u32 v[8];
+
+    static constexpr int LIMBS = 8;
+
+    ZK_DI static Fp zero() {
+        Fp r;
+#pragma unroll
+        for (int i = 0; i < 8; i++) r.v[i] = 0;
+        return r;
+    }
+    ZK_DI static Fp one() {
+        Fp r;
+#pragma unroll
+        for (int i = 0; i < 8; i++) r.v[i] = P::r1(i);
+        return r;
+    }
+    ZK_DI static Fp from_words(const u32 *w) {
+        Fp r;
+#pragma unroll
+        for (int i = 0; i < 8; i++) r.v[i] = w[i];
+        return r;
+    }
+
+    // 128-bit vector load / store of one 32-byte element
+    ZK_DI static Fp load(const u32 *p) {
+        const uint4 *q = reinterpret_cast<const uint4 *>(p);
+        uint4 a = q[0], b = q[1];
+        Fp r;
+        r.v[0] = a.x; r.v[1] = a.y; r.v[2] = a.z; r.v[3] = a.w;
+        r.v[4] = b.x; r.v[5] = b.y; r.v[6] = b.z; r.v[7] = b.w;
+        return r;
+    }
+    ZK_DI static Fp load_nc(const u32 *p) {
+        const uint4 *q = reinterpret_cast<const uint4 *>(p);
+        uint4 a = __ldg(q), b = __ldg(q + 1);
+        Fp r;
+        r.v[0] = a.x; r.v[1] = a.y; r.v[2] = a.z; r.v[3] = a.w;
+        r.v[4] = b.x; r.v[5] = b.y; r.v[6] = b.z; r.v[7] = b.w;
+        return r;
+    }
+    ZK_DI void store(u32 *p) const {
+        uint4 *q = reinterpret_cast<uint4 *>(p);
+        q[0] = make_uint4(v[0], v[1], v[2], v[3]);
+        q[1] = make_uint4(v[4], v[5], v[6], v[7]);
+    }
+
+    ZK_DI bool is_zero() const {
+        u32 acc = 0;
+#pragma unroll
+        for (int i = 0; i < 8; i++) acc |= v[i];
+        return acc == 0;
+    }
+    ZK_DI bool operator==(const Fp &o) const {
+        u32 acc = 0;
+#pragma unroll
+        for (int i = 0; i < 8; i++) acc |= v[i] ^ o.v[i];
+        return acc == 0;
+    }
+
+    // r = a - b over 256 bits; returns the borrow (0 or 1)
+    ZK_DI static u32 sub_raw(u32 *r, const u32 *a, const u32 *b) {
+        r[0] = sub_cc(a[0], b[0]);
+#pragma unroll
+        for (int i = 1; i < 8; i++) r[i] = subc_cc(a[i], b[i]);
+        return subc(0u, 0u) & 1u;
+    }
+
+    // x in [0, 2k) -> [0, k) for k = m (K2 = false) or k = 2m (K2 = true)
+    template <bool K2>
+    ZK_DI static void fold(u32 *x) {
+        u32 t[8];
+        if (K2) {
+            t[0] = sub_cc(x[0], P::m2(0));
+#pragma unroll
+            for (int i = 1; i < 8; i++) t[i] = subc_cc(x[i], P::m2(i));
+        } else {
+            t[0] = sub_cc(x[0], P::m(0));
+#pragma unroll
+            for (int i = 1; i < 8; i++) t[i] = subc_cc(x[i], P::m(i));
+        }
+        u32 borrow = subc(0u, 0u);
+        bool keep = borrow != 0;
+#pragma unroll
+        for (int i = 0; i < 8; i++) x[i] = keep ? x[i] : t[i];
+    }
+
+    // [0, 2m) -> [0, m)
+    ZK_DI Fp canonical() const {
+        Fp r = *this;
+        fold<false>(r.v);
+        return r;
+    }
+
+    // lazy add: a, b < 2m -> (a + b) mod 2m in [0, 2m)
+    ZK_DI static Fp add(const Fp &a, const Fp &b) {
+        Fp r;
+        r.v[0] = add_cc(a.v[0], b.v[0]);
+#pragma unroll
+        for (int i = 1; i < 8; i++) r.v[i] = addc_cc(a.v[i], b.v[i]);
+        fold<true>(r.v);  // a + b < 4m < 2^256, no carry out
+        return r;
+    }
+
+    // lazy sub: a, b < 2m -> (a - b) mod 2m in [0, 2m)
+    ZK_DI static Fp sub(const Fp &a, const Fp &b) {
+        Fp r;
+        u32 borrow = sub_raw(r.v, a.v, b.v);
+        u32 mask = 0u - borrow;
+        r.v[0] = add_cc(r.v[0], P::m2(0) & mask);
+#pragma unroll
+        for (int i = 1; i < 8; i++) r.v[i] = addc_cc(r.v[i], P::m2(i) & mask);
+        return r;
+    }
+
+    // canonical add / sub: inputs < m, outputs < m
+    ZK_DI static Fp add_c(const Fp &a, const Fp &b) {
+        Fp r;
+        r.v[0] = add_cc(a.v[0], b.v[0]);
+#pragma unroll
+        for (int i = 1; i < 8; i++) r.v[i] = addc_cc(a.v[i], b.v[i]);
+        fold<false>(r.v);
+        return r;
+    }
+    ZK_DI static Fp sub_c(const Fp &a, const Fp &b) {
+        Fp r;
+        u32 borrow = sub_raw(r.v, a.v, b.v);
+        u32 mask = 0u - borrow;
+        r.v[0] = add_cc(r.v[0], P::m(0) & mask);
+#pragma unroll
+        for (int i = 1; i < 8; i++) r.v[i] = addc_cc(r.v[i], P::m(i) & mask);
+        return r;
+    }
+
+    // lazy negation: a < 2m -> 2m - a, mapped so that 0 stays 0 (result in [0, 2m))
+    ZK_DI static Fp neg(const Fp &a) {
+        Fp r;
+        u32 m2[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) m2[i] = P::m2(i);
+        sub_raw(r.v, m2, a.v);
+        bool z = a.is_zero();
+#pragma unroll
+        for (int i = 0; i < 8; i++) r.v[i] = z ? 0u : r.v[i];
+        return r;
+    }
+
+    // doubling (lazy)
+    ZK_DI static Fp dbl(const Fp &a) { return add(a, a); }
+
+    // CIOS Montgomery product: a, b < 2m -> a * b / R mod m in [0, 2m)
+    ZK_DI static Fp mul(const Fp &a, const Fp &b) {
+        u32 t[9];
+        // row 0: t = a * b[0]; the low products do not overlap, the high products are
+        // added with one carry chain
+        {
+            const u32 bi = b.v[0];
+#pragma unroll
+            for (int j = 0; j < 8; j++) t[j] = a.v[j] * bi;
+            t[1] = mad_hi_cc(a.v[0], bi, t[1]);
+#pragma unroll
+            for (int j = 1; j < 7; j++) t[j + 1] = madc_hi_cc(a.v[j], bi, t[j + 1]);
+            t[8] = madc_hi(a.v[7], bi, 0u);
+            reduce_row(t);
+        }
+#pragma unroll
+        for (int i = 1; i < 8; i++) {
+            const u32 bi = b.v[i];
+            // low halves: t[0..7] += lo(a[j] * bi), carry into t[8]
+            t[0] = mad_lo_cc(a.v[0], bi, t[0]);
+#pragma unroll
+            for (int j = 1; j < 8; j++) t[j] = madc_lo_cc(a.v[j], bi, t[j]);
+            t[8] = addc(t[8], 0u);
+            // high halves: t[1..8] += hi(a[j] * bi)
+            t[1] = mad_hi_cc(a.v[0], bi, t[1]);
+#pragma unroll
+            for (int j = 1; j < 7; j++) t[j + 1] = madc_hi_cc(a.v[j], bi, t[j + 1]);
+            t[8] = madc_hi(a.v[7], bi, t[8]);
+            reduce_row(t);
+        }
+        Fp r;
+#pragma unroll
+        for (int i = 0; i < 8; i++) r.v[i] = t[i];
+        return r;
+    }
+
+    // one Montgomery reduction row: t += q * m with q = t[0] * m' (so the low word becomes
+    // zero), then t >>= 32.  The low product is never formed: its carry is (t[0] != 0).
+    ZK_DI static void reduce_row(u32 *t) {
+        const u32 q = t[0] * P::MPRIME;
+        // carry out of t[0] + lo(q * m0) == (t[0] != 0)
+        add_cc(t[0], 0xffffffffu);
+        t[1] = madc_lo_cc(q, P::m(1), t[1]);
+        t[2] = madc_lo_cc(q, P::m(2), t[2]);
+        t[3] = madc_lo_cc(q, P::m(3), t[3]);
+        t[4] = madc_lo_cc(q, P::m(4), t[4]);
+        t[5] = madc_lo_cc(q, P::m(5), t[5]);
+        t[6] = madc_lo_cc(q, P::m(6), t[6]);
+        t[7] = madc_lo_cc(q, P::m(7), t[7]);
+        t[8] = addc(t[8], 0u);
+        t[1] = mad_hi_cc(q, P::m(0), t[1]);
+        t[2] = madc_hi_cc(q, P::m(1), t[2]);
+        t[3] = madc_hi_cc(q, P::m(2), t[3]);
+        t[4] = madc_hi_cc(q, P::m(3), t[4]);
+        t[5] = madc_hi_cc(q, P::m(4), t[5]);
+        t[6] = madc_hi_cc(q, P::m(5), t[6]);
+        t[7] = madc_hi_cc(q, P::m(6), t[7]);
+        t[8] = madc_hi(q, P::m(7), t[8]);
+#pragma unroll
+        for (int j = 0; j < 8; j++) t[j] = t[j + 1];
+        t[8] = 0;
+    }
+
+    ZK_DI static Fp sqr(const Fp &a) { return mul(a, a); }
+
+    // exponentiation by a 64-bit exponent (Element::pow with a small exponent)
+    ZK_DI static Fp pow_u64(const Fp &a, u64 e) {
+        Fp r = one();
+        Fp base = a;
+        while (e) {
+            if (e & 1) r = mul(r, base);
+            base = mul(base, base);
+            e >>= 1;
+        }
+        return r;
+    }
+
+    // inverse by Fermat: a^(m-2) (Element::invert, field.cuh:1172-1175)
+    ZK_DI static Fp inv(const Fp &a) {
+        Fp r = one();
+#pragma unroll 1
+        for (int w = 7; w >= 0; w--) {
+            const u32 e = (w == 0) ? (P::m(0) - 2u) : P::m(w);
+#pragma unroll 1
+            for (int b = 31; b >= 0; b--) {
+                r = mul(r, r);
+                if ((e >> b) & 1u) r = mul(r, a);
+            }
+        }
+        return r;
+    }
+
+    // Montgomery form <-> integer
+    ZK_DI static Fp to_mont(const Fp &x) {
+        Fp r2;
+#pragma unroll
+        for (int i = 0; i < 8; i++) r2.v[i] = P::r2(i);
+        return mul(x, r2).canonical();
+    }
+    ZK_DI Fp to_number() const {
+        Fp o = zero();
+        o.v[0] = 1;
+        return mul(*this, o).canonical();
+    }
+};
+
+using Fr = Fp<FrParams>;
+using Fq = Fp<FqParams>;
+
+}  // namespace zk

@@ -1,0 +1,647 @@
+// libmsm.so: Pippenger multi-scalar multiplication over BN254 G1 for sm_100a.
+//
+// Replaces the reference's MSM (core/src/msm/src/msm.cu:9-50, msm_impl.cuh:22-909) behind
+// the same C ABI (core/src/msm/src/msm.h:4-11) and adds an asynchronous device-pointer entry
+// for resident bases.  Result: sum_i s_i * P_i as a canonical affine Montgomery point,
+// identity = (0, 0), exactly what the reference returns after to_affine (msm.cu:38).
+//
+// Pipeline (all on the device, no locks, no host arithmetic):
+//   1. digits:   each scalar leaves Montgomery form (to_number, msm_impl.cuh:52), is cut into
+//                W windows of c bits and recoded to signed digits in [-2^(c-1), 2^(c-1)]
+//                (signed_digit, msm_impl.cuh:22-33); non-zero digits count into per-bucket
+//                histograms.  With precomputed tables (reference MSMPrecompute,
+//                msm_impl.cuh:776-828) logical window j*Wp + w maps to table j, window w.
+//   2. scan:     exclusive prefix sum of the histograms gives every bucket's run.
+//   3. scatter:  digits are recomputed and each (point index, sign) lands in its bucket's run,
+//                so the array is sorted by (window, bucket) - a counting sort.
+//   4. accumulate: the sorted array is cut into equal chunks, one per thread; each thread
+//                walks its chunk with mixed additions.  Runs wholly inside a chunk are written
+//                straight to their bucket; runs cut by a chunk boundary leave partial sums that
+//                a fix-up pass joins.  Load balance does not depend on the scalar distribution.
+//   5. reduce:   per window sum_b b * S_b in parallel segments: each segment forms the running
+//                sums of its buckets (summation by parts) and adds (segment start) * segment
+//                sum; segments are then tree-summed.
+//   6. combine:  one thread folds the windows (c doublings each) and normalises to affine.
+#include <cuda_runtime.h>
+#include <dlfcn.h>
+#include <atomic>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/msm.h"
+#include "common.cuh"
+#include "curve.cuh"
+
+namespace zk {
+namespace msm {
+
+constexpr int SCALAR_BITS = 254;
+constexpr u32 EMPTY = 0xffffffffu;
+
+struct Config {
+    u64 n;          // points per table
+    u32 c;          // window bits
+    u32 W;          // logical windows = ceil(254 / c)
+    u32 n_tables;   // precomputed tables (1 = none)
+    u32 Wp;         // physical windows = ceil(W / n_tables)
+    u32 B;          // buckets per window = 2^(c-1)
+    u32 K;          // entries per accumulation chunk
+    u32 L;          // buckets per reduction segment
+};
+
+inline Config make_config(u64 n, u32 c, u32 n_tables) {
+    Config cfg{};
+    cfg.n = n;
+    cfg.c = c;
+    cfg.W = (SCALAR_BITS + c - 1) / c;
+    cfg.n_tables = n_tables;
+    cfg.Wp = (cfg.W + n_tables - 1) / n_tables;
+    cfg.B = 1u << (c - 1);
+    cfg.L = cfg.B < 16 ? cfg.B : 16;
+    // chunk so that roughly 4 waves of 384 threads per SM cover the entries
+    const u64 entries = n * cfg.W;
+    const u64 threads = (u64)num_sms() * 384 * 4;
+    u64 k = (entries + threads - 1) / threads;
+    if (k < 8) k = 8;
+    if (k > 4096) k = 4096;
+    cfg.K = (u32)k;
+    return cfg;
+}
+
+// default window width for n points (a cost model in the spirit of
+// core/src/msm/tuning/cost_model.py: n*W mixed adds vs 2*W*2^(c-1) bucket adds)
+inline u32 default_window(u64 n) {
+    u32 best = 8;
+    double best_cost = 1e300;
+    for (u32 c = 8; c <= 20; c++) {
+        const double W = (double)((SCALAR_BITS + c - 1) / c);
+        const double cost = (double)n * W * 10.0 + W * (double)(1u << (c - 1)) * 2.2 * 14.0 + W * c * 8.0 * 1000.0;
+        if (cost < best_cost) {
+            best_cost = cost;
+            best = c;
+        }
+    }
+    return best;
+}
+
+// ------------------------------------------------------------------ workspace layout
+struct Layout {
+    size_t points, scalars, counts, cursor, sorted_bucket, sorted_point, bucket_sums, part_pts, part_bucket,
+        part_flag, seg, win, result, total;
+    u64 entries, chunks, segs;
+};
+
+inline size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
+
+inline Layout make_layout(const Config &cfg, bool with_points, bool with_scalars) {
+    Layout l{};
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        size_t o = off;
+        off += align_up(bytes);
+        return o;
+    };
+    const u64 nb = (u64)cfg.Wp * cfg.B;
+    l.entries = cfg.n * cfg.W;
+    l.chunks = (l.entries + cfg.K - 1) / cfg.K;
+    l.segs = nb / cfg.L;
+    l.points = with_points ? take(cfg.n * cfg.n_tables * 64) : 0;
+    l.scalars = with_scalars ? take(cfg.n * 32) : 0;
+    l.counts = take((nb + 1) * 4);
+    l.cursor = take((nb + 1) * 4);
+    l.sorted_bucket = take(l.entries * 4);
+    l.sorted_point = take(l.entries * 4);
+    l.bucket_sums = take(nb * 128);
+    l.part_pts = take(l.chunks * 2 * 128);
+    l.part_bucket = take(l.chunks * 2 * 4);
+    l.part_flag = take(l.chunks * 2 * 4);
+    l.seg = take(l.segs * 128);
+    l.win = take((size_t)cfg.Wp * 128);
+    l.result = take(64);
+    l.total = off;
+    return l;
+}
+
+// ------------------------------------------------------------------ 1 + 3: digits
+// signed c-bit digits of the canonical scalar, least significant window first
+struct Digits {
+    u32 limbs[8];
+    u32 c;
+
+    ZK_DI u32 raw(u32 w) const {
+        const u32 bit = w * c;
+        const u32 word = bit >> 5, sh = bit & 31;
+        if (word >= 8) return 0;
+        u64 v = limbs[word];
+        if (word + 1 < 8) v |= (u64)limbs[word + 1] << 32;
+        return (u32)(v >> sh) & ((1u << c) - 1);
+    }
+};
+
+ZK_DI void load_digits(Digits &d, const u32 *scalar, u32 c) {
+    Fr s = Fr::load(scalar);
+    Fr num = s.to_number();
+#pragma unroll
+    for (int i = 0; i < 8; i++) d.limbs[i] = num.v[i];
+    d.c = c;
+}
+
+// per (scalar, window): bucket key (physical window * B + |d| - 1) and negative flag; key
+// EMPTY for a zero digit
+template <typename F>
+ZK_DI void for_each_digit(const Digits &d, const Config &cfg, F &&f) {
+    u32 carry = 0;
+    const u32 half = 1u << (cfg.c - 1);
+    for (u32 w = 0; w < cfg.W; w++) {
+        u32 raw = d.raw(w) + carry;
+        bool neg = false;
+        u32 mag;
+        if (raw > half) {
+            mag = (1u << cfg.c) - raw;
+            neg = true;
+            carry = 1;
+        } else {
+            mag = raw;
+            carry = 0;
+        }
+        if (mag != 0) {
+            const u32 table = w / cfg.Wp, pw = w % cfg.Wp;
+            f(table, pw * cfg.B + mag - 1, neg);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) count_kernel(const u32 *scalars, Config cfg, u32 *counts) {
+    const u64 stride = (u64)gridDim.x * blockDim.x;
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < cfg.n; i += stride) {
+        Digits d;
+        load_digits(d, scalars + i * 8, cfg.c);
+        for_each_digit(d, cfg, [&](u32, u32 key, bool) { atomicAdd(counts + key, 1u); });
+    }
+}
+
+__global__ void __launch_bounds__(256) scatter_kernel(const u32 *scalars, Config cfg, u32 *cursor,
+                                                     u32 *sorted_bucket, u32 *sorted_point) {
+    const u64 stride = (u64)gridDim.x * blockDim.x;
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < cfg.n; i += stride) {
+        Digits d;
+        load_digits(d, scalars + i * 8, cfg.c);
+        for_each_digit(d, cfg, [&](u32 table, u32 key, bool neg) {
+            const u32 pos = atomicAdd(cursor + key, 1u);
+            sorted_bucket[pos] = key;
+            sorted_point[pos] = (u32)(table * cfg.n + i) | (neg ? 0x80000000u : 0u);
+        });
+    }
+}
+
+// ------------------------------------------------------------------ 2: exclusive scan
+// three-phase scan of u32 counts: block sums, scan of block sums, per-block scan + offset
+constexpr u32 SCAN_BLOCK = 1024;
+constexpr u32 SCAN_ITEMS = 4;
+
+__device__ u32 block_exclusive_scan(u32 v, u32 *sm, u32 &total) {
+    const u32 lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    u32 x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        u32 y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= (u32)o) x += y;
+    }
+    if (lane == 31) sm[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        u32 s = lane < (blockDim.x >> 5) ? sm[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            u32 y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= (u32)o) s += y;
+        }
+        sm[lane] = s;
+    }
+    __syncthreads();
+    const u32 prefix = (wid > 0 ? sm[wid - 1] : 0) + x - v;
+    total = sm[(blockDim.x >> 5) - 1];
+    __syncthreads();
+    return prefix;
+}
+
+__global__ void __launch_bounds__(SCAN_BLOCK) scan_reduce_kernel(const u32 *in, u64 n, u32 *block_sums) {
+    __shared__ u32 sm[32];
+    const u64 base = (u64)blockIdx.x * SCAN_BLOCK * SCAN_ITEMS + (u64)threadIdx.x * SCAN_ITEMS;
+    u32 s = 0;
+    for (u32 k = 0; k < SCAN_ITEMS; k++)
+        if (base + k < n) s += in[base + k];
+    u32 total;
+    block_exclusive_scan(s, sm, total);
+    if (threadIdx.x == 0) block_sums[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(SCAN_BLOCK) scan_blocks_kernel(u32 *block_sums, u32 nblocks) {
+    __shared__ u32 sm[32];
+    u32 carry = 0;
+    for (u32 base = 0; base < nblocks; base += SCAN_BLOCK) {
+        const u32 i = base + threadIdx.x;
+        const u32 v = i < nblocks ? block_sums[i] : 0;
+        u32 total;
+        const u32 p = block_exclusive_scan(v, sm, total);
+        if (i < nblocks) block_sums[i] = p + carry;
+        carry += total;
+    }
+}
+
+__global__ void __launch_bounds__(SCAN_BLOCK) scan_apply_kernel(const u32 *in, u64 n, const u32 *block_sums,
+                                                               u32 *out, u32 *out2) {
+    __shared__ u32 sm[32];
+    const u64 base = (u64)blockIdx.x * SCAN_BLOCK * SCAN_ITEMS + (u64)threadIdx.x * SCAN_ITEMS;
+    u32 vals[SCAN_ITEMS];
+    u32 s = 0;
+    for (u32 k = 0; k < SCAN_ITEMS; k++) {
+        vals[k] = base + k < n ? in[base + k] : 0;
+        s += vals[k];
+    }
+    u32 total;
+    u32 p = block_exclusive_scan(s, sm, total) + block_sums[blockIdx.x];
+    for (u32 k = 0; k < SCAN_ITEMS; k++) {
+        if (base + k < n) {
+            out[base + k] = p;
+            out2[base + k] = p;
+        }
+        p += vals[k];
+    }
+}
+
+// ------------------------------------------------------------------ 4: accumulation
+ZK_DI G1A fetch_point(const u32 *points, u32 code) {
+    const u32 idx = code & 0x7fffffffu;
+    G1A p = G1A::load_nc(points + (u64)idx * 16);
+    if (code & 0x80000000u) p = p.neg();
+    return p;
+}
+
+// part_flag: 1 = head run (continued from the previous chunk, ends here), 2 = head run that
+// also continues into the next chunk, 3 = tail run (starts here, continues into the next)
+__global__ void __launch_bounds__(256) accumulate_kernel(const u32 *points, const u32 *sorted_bucket,
+                                                        const u32 *sorted_point, const u32 *live, u32 K,
+                                                        u32 *bucket_sums, u32 *part_pts, u32 *part_bucket,
+                                                        u32 *part_flag) {
+    const u64 entries = *live;
+    const u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    const u64 start = t * K;
+    if (start >= entries) return;
+    const u64 end = start + K < entries ? start + K : entries;
+    const bool from_prev = start > 0 && sorted_bucket[start - 1] == sorted_bucket[start];
+    u64 run_start = start;
+    u32 cur = sorted_bucket[start];
+    G1X acc = G1X::from_affine(fetch_point(points, sorted_point[start]));
+    for (u64 p = start + 1; p <= end; p++) {
+        const u32 b = p < end ? sorted_bucket[p] : EMPTY;
+        if (p < end && b == cur) {
+            acc = g1_madd(acc, fetch_point(points, sorted_point[p]));
+            continue;
+        }
+        // the run [run_start, p) of bucket `cur` ends here
+        const bool head = run_start == start && from_prev;
+        const bool to_next = p == end && end < entries && sorted_bucket[end] == cur;
+        if (!head && !to_next) {
+            acc.store(bucket_sums + (u64)cur * 32);
+        } else {
+            const u64 slot = head ? 2 * t : 2 * t + 1;
+            acc.store(part_pts + slot * 32);
+            part_bucket[slot] = cur;
+            part_flag[slot] = head ? (to_next ? 2u : 1u) : 3u;
+        }
+        if (p < end) {
+            cur = b;
+            run_start = p;
+            acc = G1X::from_affine(fetch_point(points, sorted_point[p]));
+        }
+    }
+}
+
+// joins the partial sums of every run that crosses chunk boundaries
+__global__ void __launch_bounds__(256) fixup_kernel(const u32 *live, u32 K, u32 *bucket_sums, const u32 *part_pts,
+                                                   const u32 *part_bucket, const u32 *part_flag) {
+    const u64 chunks = ((u64)*live + K - 1) / K;
+    const u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= chunks || part_flag[2 * t + 1] != 3u) return;
+    const u64 slot = 2 * t + 1;
+    const u32 bucket = part_bucket[slot];
+    G1X acc = G1X::load(part_pts + slot * 32);
+    for (u64 u = t + 1; u < chunks; u++) {
+        const u32 f = part_flag[2 * u];
+        if ((f != 1u && f != 2u) || part_bucket[2 * u] != bucket) break;
+        acc = g1_add(acc, G1X::load(part_pts + 2 * u * 32));
+        if (f == 1u) break;
+    }
+    acc.store(bucket_sums + (u64)bucket * 32);
+}
+
+// ------------------------------------------------------------------ 5: bucket reduction
+// segment g of window w covers buckets b = g*L + 1 .. g*L + L (stored at index b - 1):
+// out = sum_j (g*L + j + 1) * S[g*L + j] = runsum-weighted part + (g*L) * plain sum
+__global__ void __launch_bounds__(128) segment_kernel(const u32 *bucket_sums, u32 B, u32 L, u64 segs, u32 *seg_out) {
+    const u64 s = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= segs) return;
+    const u64 segs_per_window = B / L;
+    const u64 g = s % segs_per_window;
+    const u32 *base = bucket_sums + s * L * 32;
+    G1X run = G1X::identity(), acc = G1X::identity();
+    for (int j = (int)L - 1; j >= 0; j--) {
+        run = g1_add(run, G1X::load(base + (u64)j * 32));
+        acc = g1_add(acc, run);
+    }
+    if (g > 0) acc = g1_add(acc, g1_mul_u64(run, g * L));
+    acc.store(seg_out + s * 32);
+}
+
+// per window: tree-sum of its segments (one CTA per window)
+__global__ void __launch_bounds__(256) window_sum_kernel(const u32 *seg_out, u64 segs_per_window, u32 *win_out) {
+    __shared__ u32 sm[256 * 32];
+    const u32 w = blockIdx.x;
+    const u32 *base = seg_out + (u64)w * segs_per_window * 32;
+    G1X acc = G1X::identity();
+    for (u64 i = threadIdx.x; i < segs_per_window; i += blockDim.x) acc = g1_add(acc, G1X::load(base + i * 32));
+    acc.store(sm + threadIdx.x * 32);
+    __syncthreads();
+    for (u32 stride = blockDim.x / 2; stride > 0; stride >>= 1) {
+        if (threadIdx.x < stride) {
+            G1X a = G1X::load(sm + threadIdx.x * 32);
+            G1X b = G1X::load(sm + (threadIdx.x + stride) * 32);
+            g1_add(a, b).store(sm + threadIdx.x * 32);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) G1X::load(sm).store(win_out + (u64)w * 32);
+}
+
+// ------------------------------------------------------------------ 6: window combination
+__global__ void combine_kernel(const u32 *win_out, u32 Wp, u32 c, u32 *result) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    G1X acc = G1X::load(win_out + (u64)(Wp - 1) * 32);
+    for (int w = (int)Wp - 2; w >= 0; w--) {
+        for (u32 k = 0; k < c; k++) acc = g1_dbl(acc);
+        acc = g1_add(acc, G1X::load(win_out + (u64)w * 32));
+    }
+    g1_to_affine(acc).store(result);
+}
+
+// ------------------------------------------------------------------ precompute tables
+// table j = 2^(j * Wp * c) * P, affine (MSMPrecompute::run, msm_impl.cuh:776-800)
+__global__ void __launch_bounds__(128) precompute_kernel(const u32 *src, u32 *dst, u64 n, u32 shift_bits) {
+    const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    G1X p = G1X::from_affine(G1A::load(src + i * 16));
+    for (u32 k = 0; k < shift_bits; k++) p = g1_dbl(p);
+    g1_to_affine(p).store(dst + i * 16);
+}
+
+__global__ void add_points_kernel(u32 *acc_affine, const u32 *other_affine) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    G1X a = G1X::from_affine(G1A::load(acc_affine));
+    a = g1_madd(a, G1A::load(other_affine));
+    g1_to_affine(a).store(acc_affine);
+}
+
+// ------------------------------------------------------------------ driver
+inline u32 grid_for(u64 items, u32 block, u32 per_sm = 8) {
+    const u64 b = (items + block - 1) / block;
+    const u64 cap = (u64)num_sms() * per_sm;
+    return (u32)(b < cap ? (b == 0 ? 1 : b) : cap);
+}
+
+// Runs one MSM with points / scalars already on the device; `ws` holds the layout regions.
+cudaError_t run_device(const Config &cfg, const Layout &l, char *ws, const u32 *d_points, const u32 *d_scalars,
+                       u32 *d_result, cudaStream_t stream) {
+    const u64 nb = (u64)cfg.Wp * cfg.B;
+    u32 *counts = reinterpret_cast<u32 *>(ws + l.counts);
+    u32 *cursor = reinterpret_cast<u32 *>(ws + l.cursor);
+    u32 *sb = reinterpret_cast<u32 *>(ws + l.sorted_bucket);
+    u32 *sp = reinterpret_cast<u32 *>(ws + l.sorted_point);
+    u32 *bs = reinterpret_cast<u32 *>(ws + l.bucket_sums);
+    u32 *pp = reinterpret_cast<u32 *>(ws + l.part_pts);
+    u32 *pb = reinterpret_cast<u32 *>(ws + l.part_bucket);
+    u32 *pf = reinterpret_cast<u32 *>(ws + l.part_flag);
+    u32 *seg = reinterpret_cast<u32 *>(ws + l.seg);
+    u32 *win = reinterpret_cast<u32 *>(ws + l.win);
+
+    ZK_TRY(cudaMemsetAsync(counts, 0, (nb + 1) * 4, stream));
+    ZK_TRY(cudaMemsetAsync(bs, 0, nb * 128, stream));
+    ZK_TRY(cudaMemsetAsync(pf, 0, l.chunks * 2 * 4, stream));
+    count_kernel<<<grid_for(cfg.n, 256), 256, 0, stream>>>(d_scalars, cfg, counts);
+    ZK_TRY(cudaGetLastError());
+    // exclusive scan of the nb + 1 counters: cursor[k] = first slot of bucket k, and
+    // counts[nb] becomes the number of live (non-zero digit) entries
+    const u64 items = nb + 1;
+    const u32 nblocks = (u32)((items + SCAN_BLOCK * SCAN_ITEMS - 1) / (SCAN_BLOCK * SCAN_ITEMS));
+    u32 *block_sums = seg;  // the segment buffer is free until the reduction
+    scan_reduce_kernel<<<nblocks, SCAN_BLOCK, 0, stream>>>(counts, items, block_sums);
+    scan_blocks_kernel<<<1, SCAN_BLOCK, 0, stream>>>(block_sums, nblocks);
+    scan_apply_kernel<<<nblocks, SCAN_BLOCK, 0, stream>>>(counts, items, block_sums, cursor, counts);
+    ZK_TRY(cudaGetLastError());
+    scatter_kernel<<<grid_for(cfg.n, 256), 256, 0, stream>>>(d_scalars, cfg, cursor, sb, sp);
+    ZK_TRY(cudaGetLastError());
+    const u32 *live = counts + nb;
+    accumulate_kernel<<<(u32)((l.chunks + 255) / 256), 256, 0, stream>>>(d_points, sb, sp, live, cfg.K, bs, pp, pb,
+                                                                         pf);
+    ZK_TRY(cudaGetLastError());
+    fixup_kernel<<<(u32)((l.chunks + 255) / 256), 256, 0, stream>>>(live, cfg.K, bs, pp, pb, pf);
+    ZK_TRY(cudaGetLastError());
+    segment_kernel<<<(u32)((l.segs + 127) / 128), 128, 0, stream>>>(bs, cfg.B, cfg.L, l.segs, seg);
+    ZK_TRY(cudaGetLastError());
+    window_sum_kernel<<<cfg.Wp, 256, 0, stream>>>(seg, cfg.B / cfg.L, win);
+    ZK_TRY(cudaGetLastError());
+    combine_kernel<<<1, 32, 0, stream>>>(win, cfg.Wp, cfg.c, d_result);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ library configuration
+// The reference builds one libmsm_<curve>_<s>_<target_windows>_<debug>.so per configuration
+// (core/src/msm.rs:100-111) with the number of precomputed point tables fixed at compile time
+// (msm.cuh:53-69).  This library reads the same fields from its own file name when it is
+// installed under such a name, so a caller passes exactly as many tables as it would to the
+// reference; under any other name there is one table and the window is chosen per call.
+struct LibConfig {
+    u32 window = 0;   // 0 = choose per call
+    u32 target_windows = 0;
+};
+
+inline LibConfig lib_config() {
+    static LibConfig cfg;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        Dl_info info;
+        if (dladdr(reinterpret_cast<void *>(&lib_config), &info) && info.dli_fname) {
+            std::string name(info.dli_fname);
+            auto slash = name.find_last_of('/');
+            if (slash != std::string::npos) name = name.substr(slash + 1);
+            unsigned s = 0, tw = 0;
+            char curve[32] = {0}, dbg[16] = {0};
+            if (sscanf(name.c_str(), "libmsm_%31[a-z0-9]_%u_%u_%15[a-z]", curve, &s, &tw, dbg) == 4 && s >= 2 &&
+                s <= 24 && tw >= 1) {
+                cfg.window = s;
+                cfg.target_windows = tw;
+            }
+        }
+    });
+    return cfg;
+}
+
+inline void resolve(u64 n, u32 window, u32 n_tables_hint, u32 *c, u32 *n_tables) {
+    LibConfig lc = lib_config();
+    u32 cc = window ? window : (lc.window ? lc.window : default_window(n));
+    u32 W = (SCALAR_BITS + cc - 1) / cc;
+    u32 nt = 1;
+    if (n_tables_hint) {
+        nt = n_tables_hint;
+    } else if (lc.target_windows) {
+        u32 nw = W < lc.target_windows ? W : lc.target_windows;
+        nt = (W + nw - 1) / nw;
+    }
+    *c = cc;
+    *n_tables = nt;
+}
+
+}  // namespace msm
+}  // namespace zk
+
+using namespace zk;
+
+extern "C" unsigned int zkp_msm_default_window(unsigned long long n) { return msm::default_window(n); }
+
+extern "C" unsigned long long zkp_msm_workspace_size(unsigned long long n, unsigned int window, unsigned int n_tables) {
+    u32 c, nt;
+    msm::resolve(n, window, n_tables, &c, &nt);
+    return msm::make_layout(msm::make_config(n, c, nt), false, false).total;
+}
+
+extern "C" cudaError_t zkp_msm_device(void *workspace_d, unsigned long long workspace_bytes,
+                                      const unsigned int *points_d, unsigned int n_tables,
+                                      const unsigned int *scalars_d, unsigned long long n, unsigned int window,
+                                      unsigned int *result_d, cudaStream_t stream) {
+    ZK_CHECK_ARG(result_d != nullptr);
+    if (n == 0) return cudaMemsetAsync(result_d, 0, 64, stream);
+    ZK_CHECK_ARG(points_d != nullptr && scalars_d != nullptr && workspace_d != nullptr);
+    u32 c, nt;
+    msm::resolve(n, window, n_tables, &c, &nt);
+    ZK_CHECK_ARG(c >= 2 && c <= 24 && nt >= 1);
+    ZK_CHECK_ARG(n * nt < (1ull << 31));
+    msm::Config cfg = msm::make_config(n, c, nt);
+    msm::Layout l = msm::make_layout(cfg, false, false);
+    ZK_CHECK_ARG(workspace_bytes >= l.total);
+    return msm::run_device(cfg, l, reinterpret_cast<char *>(workspace_d), points_d, scalars_d, result_d, stream);
+}
+
+extern "C" cudaError_t zkp_msm_precompute_device(unsigned int *tables_d, unsigned long long n, unsigned int window,
+                                                 unsigned int n_tables, cudaStream_t stream) {
+    ZK_CHECK_ARG(tables_d != nullptr && n_tables >= 1 && window >= 2 && window <= 24);
+    const u32 W = (msm::SCALAR_BITS + window - 1) / window;
+    const u32 Wp = (W + n_tables - 1) / n_tables;
+    for (u32 j = 1; j < n_tables; j++) {
+        msm::precompute_kernel<<<(u32)((n + 127) / 128), 128, 0, stream>>>(tables_d + (j - 1) * n * 16,
+                                                                           tables_d + j * n * 16, n, Wp * window);
+        ZK_TRY(cudaGetLastError());
+    }
+    return cudaSuccess;
+}
+
+extern "C" cudaError_t msm(void *const *buffers, unsigned long *buffer_sizes, unsigned long long len,
+                           unsigned int batch_per_run, unsigned int parts, unsigned int stage_scalers,
+                           unsigned int stage_points, unsigned int num_cards, const unsigned int *cards,
+                           unsigned int const *const *h_points, unsigned int batches,
+                           unsigned int const *const *h_scaler_batch, unsigned int *const *h_result) {
+    (void)batch_per_run;
+    (void)parts;
+    (void)stage_scalers;
+    (void)stage_points;
+    ZK_CHECK_ARG(num_cards >= 1 && cards != nullptr && len > 0);
+    u32 c, nt;
+    msm::resolve(len / num_cards + 1, 0, 0, &c, &nt);
+    // card k takes points [k*len/num_cards, (k+1)*len/num_cards)
+    auto slice = [&](u32 k, u64 *lo, u64 *cnt) {
+        *lo = len * k / num_cards;
+        *cnt = len * (k + 1) / num_cards - *lo;
+    };
+    if (buffers == nullptr) {
+        ZK_CHECK_ARG(buffer_sizes != nullptr);
+        for (u32 k = 0; k < num_cards; k++) {
+            u64 lo, cnt;
+            slice(k, &lo, &cnt);
+            msm::Config cfg = msm::make_config(cnt ? cnt : 1, c, nt);
+            buffer_sizes[k] = msm::make_layout(cfg, true, true).total;
+        }
+        return cudaSuccess;
+    }
+    ZK_CHECK_ARG(h_points != nullptr && (batches == 0 || (h_scaler_batch != nullptr && h_result != nullptr)));
+    int prev_dev = 0;
+    ZK_TRY(cudaGetDevice(&prev_dev));
+    std::vector<std::vector<u32>> partial(num_cards, std::vector<u32>((size_t)batches * 16, 0));
+    cudaError_t err = cudaSuccess;
+    for (u32 k = 0; k < num_cards && err == cudaSuccess; k++) {
+        u64 lo, cnt;
+        slice(k, &lo, &cnt);
+        if (cnt == 0) continue;
+        err = cudaSetDevice((int)cards[k]);
+        if (err != cudaSuccess) break;
+        msm::Config cfg = msm::make_config(cnt, c, nt);
+        msm::Layout l = msm::make_layout(cfg, true, true);
+        char *ws = reinterpret_cast<char *>(buffers[k]);
+        u32 *d_points = reinterpret_cast<u32 *>(ws + l.points);
+        u32 *d_scalars = reinterpret_cast<u32 *>(ws + l.scalars);
+        u32 *d_result = reinterpret_cast<u32 *>(ws + l.result);
+        cudaStream_t st = cudaStreamPerThread;
+        for (u32 j = 0; j < nt && err == cudaSuccess; j++)
+            err = cudaMemcpyAsync(d_points + j * cnt * 16, h_points[j] + lo * 16, cnt * 64, cudaMemcpyHostToDevice, st);
+        for (u32 b = 0; b < batches && err == cudaSuccess; b++) {
+            err = cudaMemcpyAsync(d_scalars, h_scaler_batch[b] + lo * 8, cnt * 32, cudaMemcpyHostToDevice, st);
+            if (err == cudaSuccess) err = msm::run_device(cfg, l, ws, d_points, d_scalars, d_result, st);
+            if (err == cudaSuccess)
+                err = cudaMemcpyAsync(partial[k].data() + b * 16, d_result, 64, cudaMemcpyDeviceToHost, st);
+        }
+        if (err == cudaSuccess) err = cudaStreamSynchronize(st);
+    }
+    // add the other cards' affine partials on the first card (msm_impl.cuh:902-907 does this
+    // on the host; here it is one device addition per card)
+    if (err == cudaSuccess && num_cards > 1) {
+        err = cudaSetDevice((int)cards[0]);
+        u64 lo0, cnt0;
+        slice(0, &lo0, &cnt0);
+        msm::Config cfg0 = msm::make_config(cnt0 ? cnt0 : 1, c, nt);
+        msm::Layout l0 = msm::make_layout(cfg0, true, true);
+        u32 *acc = reinterpret_cast<u32 *>(reinterpret_cast<char *>(buffers[0]) + l0.result);
+        u32 *other = acc + 16;  // the 256-byte aligned result slot has room for a second point
+        for (u32 b = 0; b < batches && err == cudaSuccess; b++) {
+            err = cudaMemcpy(acc, partial[0].data() + b * 16, 64, cudaMemcpyHostToDevice);
+            for (u32 k = 1; k < num_cards && err == cudaSuccess; k++) {
+                err = cudaMemcpy(other, partial[k].data() + b * 16, 64, cudaMemcpyHostToDevice);
+                if (err == cudaSuccess) {
+                    msm::add_points_kernel<<<1, 32>>>(acc, other);
+                    err = cudaGetLastError();
+                }
+            }
+            if (err == cudaSuccess) err = cudaMemcpy(partial[0].data() + b * 16, acc, 64, cudaMemcpyDeviceToHost);
+        }
+    }
+    if (err == cudaSuccess)
+        for (u32 b = 0; b < batches; b++) memcpy(h_result[b], partial[0].data() + b * 16, 64);
+    cudaSetDevice(prev_dev);
+    return err;
+}
+
+extern "C" cudaError_t msm_precompute(unsigned long long len, unsigned int *const *h_points, unsigned int max_cards) {
+    (void)max_cards;
+    u32 c, nt;
+    msm::resolve(len, 0, 0, &c, &nt);
+    if (nt <= 1) return cudaSuccess;
+    ZK_CHECK_ARG(h_points != nullptr && len > 0);
+    u32 *d = nullptr;
+    ZK_TRY(cudaMalloc(&d, (size_t)len * nt * 64));
+    cudaError_t err = cudaMemcpy(d, h_points[0], len * 64, cudaMemcpyHostToDevice);
+    if (err == cudaSuccess) err = zkp_msm_precompute_device(d, len, c, nt, 0);
+    for (u32 j = 1; j < nt && err == cudaSuccess; j++)
+        err = cudaMemcpy(h_points[j], d + (u64)j * len * 16, len * 64, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    return err;
+}

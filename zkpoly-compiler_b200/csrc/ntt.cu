@@ -1,0 +1,475 @@
+// libntt.so: in-place natural-order NTT over BN254 Fr for sm_100a.
+//
+// Replaces the reference's SSIP kernels (core/src/ntt/src/ssip_ntt.cuh:10-566,
+// recompute_ntt.cuh:23-438) behind the same C ABI (core/src/ntt/src/ntt.h:5-16).
+//
+// Algorithm (n = 2^L).  The index bits are split into digits of at most 12 bits, top digit
+// first.  Pass p takes every "pencil" of 2^D elements that differ only in digit p (bits
+// [lo, lo + D)), runs a radix-2 DIF sub-transform on it in shared memory (its output lands
+// bit-reversed inside the digit), and, when lower digits remain, multiplies element k of the
+// sub-transform by the four-step twist w_N^(c*k), where c is the pencil's value of the lower
+// digits and N = 2^(lo + D).  After the last digit the whole vector is in bit-reversed order;
+// a final in-place permutation pass swaps i <-> rev(i).  For L <= 12 one CTA does the whole
+// transform and writes natural order directly.
+//
+// Every pass reads and writes the same pencil, so all passes run in place on the caller's
+// buffer with no scratch memory.  Intermediate values stay in [0, 2m) (lazy Montgomery);
+// the last transform pass stores canonical values.
+//
+// Shared memory holds the pencil as 8 word planes (element e, word w at w*S + swz(e)) and the
+// 2^(D-1) sub-transform roots the same way; both swizzles keep a warp's 32 accesses on 32
+// different banks for every butterfly span.
+#include <cuda_runtime.h>
+#include <atomic>
+#include <cstring>
+#include <vector>
+
+#include "../../include/ntt.h"
+#include "common.cuh"
+#include "host_field.h"
+
+namespace zk {
+namespace ntt {
+
+constexpr u32 MAX_D = 12;
+constexpr u32 MAX_THREADS = 1024;
+
+enum Flags : u32 {
+    F_TWIST = 1u,          // multiply by the four-step twist after the sub-transform
+    F_NATURAL = 2u,        // single-pass plan: store in natural order
+    F_CANON = 4u,          // store canonical values (last transform pass)
+    F_PRESHIFT = 8u,       // multiply x[i] by shift^i on load (pass 0 only)
+    F_POSTSCALE = 16u,     // multiply by *scale on the final store
+    F_RECOMPUTE = 32u,     // derive roots from omegas[] instead of a table
+    F_SRC = 64u,           // pass 0 reads from src (zero beyond src_len), writes to v
+};
+
+struct PassArgs {
+    View v;                 // data (in place)
+    View src;               // optional source of pass 0 (coset LDE)
+    const u32 *tw;          // [w^0 .. w^(n/2-1)] (table mode)
+    const u32 *omegas;      // [w^(2^i)] (recompute mode)
+    const u32 *shift;       // coset shift (Montgomery) or null
+    const u32 *scale;       // post-scale or null
+    u32 L, D, lo, flags;
+    u64 src_len;
+};
+
+ZK_DI u32 swz(u32 e) { return e ^ (((e >> 5) & 1u) * 31u); }
+ZK_DI u32 swt(u32 x) { return x ^ (((x >> 5) ^ (x >> 10)) & 31u); }
+
+ZK_DI Fr sm_load(const u32 *base, u32 stride, u32 pos) {
+    Fr r;
+#pragma unroll
+    for (int w = 0; w < 8; w++) r.v[w] = base[w * stride + pos];
+    return r;
+}
+ZK_DI void sm_store(u32 *base, u32 stride, u32 pos, const Fr &x) {
+#pragma unroll
+    for (int w = 0; w < 8; w++) base[w * stride + pos] = x.v[w];
+}
+
+// w^e for a 64-bit exponent from the n/2 root table (w^(n/2) = -1)
+ZK_DI Fr table_root(const u32 *tw, u64 e, u32 L) {
+    const u64 half = 1ull << (L - 1);
+    if (e < half) return Fr::load_nc(tw + e * 8);
+    Fr w = Fr::load_nc(tw + (e - half) * 8);
+    return Fr::neg(w);
+}
+
+// w^e from omegas[i] = w^(2^i) (recompute mode): one multiply per set bit
+ZK_DI Fr omega_pow(const u32 *omegas, u64 e) {
+    Fr r = Fr::one();
+    int i = 0;
+    while (e) {
+        if (e & 1) r = Fr::mul(r, Fr::load_nc(omegas + i * 8));
+        e >>= 1;
+        i++;
+    }
+    return r;
+}
+
+__global__ void __launch_bounds__(MAX_THREADS, 1) ntt_pass_kernel(PassArgs a) {
+    extern __shared__ u32 sm[];
+    const u32 D = a.D;
+    const u32 S = 1u << D;
+    const u32 H = S >> 1;
+    u32 *data = sm;
+    u32 *tws = sm + 8 * S;
+    u32 *aux = tws + 8 * (H > 0 ? H : 1);  // 2 x 64 elements of shift tables (recompute twist)
+    const u32 T = blockDim.x;
+    const u32 tid = threadIdx.x;
+    const u64 P = (u64)blockIdx.y * gridDim.x + blockIdx.x;
+    const u64 cmask = (1ull << a.lo) - 1;
+    const u64 c = P & cmask;
+    const u64 h = P >> a.lo;
+    const u64 gbase = (h << (a.lo + D)) | c;
+    const bool recompute = (a.flags & F_RECOMPUTE) != 0;
+
+    // ---- sub-transform roots w_{2^D}^i, i < H
+    if (!recompute) {
+        for (u32 i = tid; i < H; i += T) {
+            Fr w = Fr::load_nc(a.tw + ((u64)i << (a.L - D)) * 8);
+            sm_store(tws, H, swt(i), w);
+        }
+    } else if (H > 0) {
+        // two-level: w^i = w^(i & 63) * w^(64 * (i >> 6)); the 64 + H/64 seeds by pow
+        const u32 lo_n = H < 64 ? H : 64;
+        const u32 hi_n = H > 64 ? H / 64 : 1;
+        for (u32 i = tid; i < lo_n + hi_n; i += T) {
+            u64 e = i < lo_n ? (u64)i : (u64)(i - lo_n) * 64;
+            Fr w = omega_pow(a.omegas, e << (a.L - D));
+            sm_store(aux, 128, i, w);
+        }
+        __syncthreads();
+        for (u32 i = tid; i < H; i += T) {
+            Fr w = sm_load(aux, 128, i & 63);
+            if (i >= 64) w = Fr::mul(w, sm_load(aux, 128, lo_n + (i >> 6)));
+            sm_store(tws, H, swt(i), w);
+        }
+        __syncthreads();
+    }
+
+    // ---- coset shift tables (pass 0): shift^(c + r*2^lo) = (shift^c * G^(r&63)) * G^(64*(r>>6))
+    const bool preshift = (a.flags & F_PRESHIFT) != 0;
+    if (preshift) {
+        if (tid < 128) {
+            Fr g = Fr::load_nc(a.shift);
+            Fr G = g;
+            for (u32 k = 0; k < a.lo; k++) G = Fr::mul(G, G);
+            Fr w;
+            if (tid < 64) {
+                w = Fr::mul(Fr::pow_u64(g, c), Fr::pow_u64(G, tid));
+            } else {
+                w = Fr::pow_u64(G, (u64)(tid - 64) * 64);
+            }
+            sm_store(aux, 128, tid, w);
+        }
+        __syncthreads();
+    }
+
+    // ---- load the pencil
+    const bool from_src = (a.flags & F_SRC) != 0;
+    for (u32 r = tid; r < S; r += T) {
+        const u64 gi = gbase + ((u64)r << a.lo);
+        Fr x;
+        if (from_src) {
+            x = gi < a.src_len ? Fr::load(a.src.at(gi)) : Fr::zero();
+        } else {
+            x = Fr::load(a.v.at(gi));
+        }
+        if (preshift) {
+            x = Fr::mul(x, sm_load(aux, 128, r & 63));
+            if (r >= 64) x = Fr::mul(x, sm_load(aux, 128, 64 + (r >> 6)));
+        }
+        sm_store(data, S, swz(r), x);
+    }
+    __syncthreads();
+
+    // ---- radix-2 DIF stages, span 2^b
+    for (int b = (int)D - 1; b >= 0; b--) {
+        const u32 hh = 1u << b;
+        for (u32 j = tid; j < H; j += T) {
+            const u32 e0 = ((j >> b) << (b + 1)) | (j & (hh - 1));
+            const u32 e1 = e0 + hh;
+            const u32 p0 = swz(e0), p1 = swz(e1);
+            Fr x0 = sm_load(data, S, p0);
+            Fr x1 = sm_load(data, S, p1);
+            Fr s = Fr::add(x0, x1);
+            Fr d = Fr::sub(x0, x1);
+            if (b > 0) {
+                const u32 ti = (j & (hh - 1)) << (D - 1 - b);
+                d = Fr::mul(d, sm_load(tws, H, swt(ti)));
+            }
+            sm_store(data, S, p0, s);
+            sm_store(data, S, p1, d);
+        }
+        __syncthreads();
+    }
+
+    // ---- twist (recompute mode: per-CTA tables of (w_N^c)^k)
+    const bool twist = (a.flags & F_TWIST) != 0;
+    if (twist && recompute) {
+        // base = w_N^c with w_N = w^(2^(L-lo-D)); tables base^(k & 63), base^(64 * (k >> 6))
+        if (tid < 128) {
+            Fr base = omega_pow(a.omegas, c << (a.L - a.lo - D));
+            Fr w = tid < 64 ? Fr::pow_u64(base, tid) : Fr::pow_u64(base, (u64)(tid - 64) * 64);
+            sm_store(aux, 128, tid, w);
+        }
+        __syncthreads();
+    }
+
+    const bool natural = (a.flags & F_NATURAL) != 0;
+    const bool canon = (a.flags & F_CANON) != 0;
+    const bool postscale = (a.flags & F_POSTSCALE) != 0;
+    Fr scale;
+    if (postscale) scale = Fr::load_nc(a.scale);
+    for (u32 q = tid; q < S; q += T) {
+        // natural: thread writes global position q, which holds smem position rev(q)
+        const u32 s = natural ? (__brev(q) >> (32 - D)) : q;
+        Fr x = sm_load(data, S, swz(s));
+        if (twist) {
+            const u32 k = __brev(s) >> (32 - D);  // natural output index of position s
+            if (c != 0 && k != 0) {
+                Fr w;
+                if (recompute) {
+                    w = sm_load(aux, 128, k & 63);
+                    if (k >= 64) w = Fr::mul(w, sm_load(aux, 128, 64 + (k >> 6)));
+                } else {
+                    const u64 e = ((u64)c * k) << (a.L - a.lo - D);
+                    w = table_root(a.tw, e, a.L);
+                }
+                x = Fr::mul(x, w);
+            }
+        }
+        if (postscale) x = Fr::mul(x, scale);
+        if (canon) x = x.canonical();
+        const u64 gi = gbase + ((u64)q << a.lo);
+        x.store(a.v.at(gi));
+    }
+}
+
+// in-place bit-reversal permutation of L index bits
+__global__ void __launch_bounds__(256) bitrev_kernel(View v, u32 L, u64 n) {
+    const u64 stride = (u64)gridDim.x * blockDim.x;
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const u64 j = __brevll(i) >> (64 - L);
+        if (i < j) {
+            u32 *pi = v.at(i), *pj = v.at(j);
+            Fr a = Fr::load(pi), b = Fr::load(pj);
+            b.store(pi);
+            a.store(pj);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) distribute_powers_kernel(View v, const u32 *powers, u64 pn, u64 n) {
+    const u64 stride = (u64)gridDim.x * blockDim.x;
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const u64 k = pn >= n ? i : ((pn & (pn - 1)) == 0 ? (i & (pn - 1)) : i % pn);
+        u32 *p = v.at(i);
+        Fr x = Fr::mul(Fr::load(p), Fr::load_nc(powers + k * 8)).canonical();
+        x.store(p);
+    }
+}
+
+// table[i] = w^i for i < len; each thread seeds w^(64 t) and walks 64 steps
+__global__ void __launch_bounds__(256) powers_kernel(u32 *out, const u32 *unit, u64 len) {
+    const u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    const u64 start = t * 64;
+    if (start >= len) return;
+    Fr w = Fr::load(unit);
+    Fr x = Fr::pow_u64(w, start);
+    const u64 end = start + 64 < len ? start + 64 : len;
+    for (u64 i = start; i < end; i++) {
+        x.canonical().store(out + i * 8);
+        x = Fr::mul(x, w);
+    }
+}
+
+// ------------------------------------------------------------------ host plan
+struct Plan {
+    u32 np;
+    u32 D[4];
+    u32 lo[4];
+};
+
+inline Plan make_plan(u32 L) {
+    Plan p{};
+    if (L <= MAX_D) {
+        p.np = 1;
+        p.D[0] = L;
+        p.lo[0] = 0;
+        return p;
+    }
+    p.np = (L + MAX_D - 1) / MAX_D;
+    u32 base = L / p.np, extra = L % p.np;
+    u32 rem = L;
+    for (u32 i = 0; i < p.np; i++) {
+        p.D[i] = base + (i < extra ? 1 : 0);
+        rem -= p.D[i];
+        p.lo[i] = rem;
+    }
+    return p;
+}
+
+std::atomic<uint64_t> g_attr_done{0};
+
+inline size_t pass_smem(u32 D) {
+    const size_t S = 1u << D, H = S > 1 ? S / 2 : 1;
+    return (8 * S + 8 * H + 8 * 128) * sizeof(u32);
+}
+
+cudaError_t launch_pass(const PassArgs &a, cudaStream_t stream) {
+    ZK_TRY(ensure_smem_attr(ntt_pass_kernel, (int)pass_smem(MAX_D), g_attr_done));
+    const u64 pencils = 1ull << (a.L - a.D);
+    const u32 H = (1u << a.D) >> 1;
+    const u32 threads = H == 0 ? 1 : (H < MAX_THREADS ? H : MAX_THREADS);
+    dim3 grid;
+    if (pencils <= 65535ull * 1024) {
+        grid.x = (u32)(pencils < 65535 ? pencils : 65535);
+        grid.y = (u32)((pencils + grid.x - 1) / grid.x);
+        if ((u64)grid.x * grid.y != pencils) {
+            // pencils is a power of two, so choose x as a power of two too
+            u32 gx = 1;
+            while ((u64)gx * 2 <= pencils && gx * 2 <= 32768) gx *= 2;
+            grid.x = gx;
+            grid.y = (u32)(pencils / gx);
+        }
+    } else {
+        return cudaErrorInvalidValue;
+    }
+    ntt_pass_kernel<<<grid, threads, pass_smem(a.D), stream>>>(a);
+    return cudaGetLastError();
+}
+
+// Runs the full plan.  src (if non-null) is the pass-0 source for the coset LDE.
+cudaError_t run(const View &v, const View *src, u64 src_len, u32 L, const u32 *tw, const u32 *omegas,
+                const u32 *shift, const u32 *scale, cudaStream_t stream) {
+    const Plan plan = make_plan(L);
+    for (u32 p = 0; p < plan.np; p++) {
+        PassArgs a{};
+        a.v = v;
+        if (src) a.src = *src;
+        a.tw = tw;
+        a.omegas = omegas;
+        a.shift = shift;
+        a.scale = scale;
+        a.L = L;
+        a.D = plan.D[p];
+        a.lo = plan.lo[p];
+        a.src_len = src_len;
+        u32 f = 0;
+        if (a.lo > 0) f |= F_TWIST;
+        if (plan.np == 1) f |= F_NATURAL;
+        if (p + 1 == plan.np) {
+            f |= F_CANON;
+            if (scale) f |= F_POSTSCALE;
+        }
+        if (p == 0 && shift) f |= F_PRESHIFT;
+        if (p == 0 && src) f |= F_SRC;
+        if (omegas) f |= F_RECOMPUTE;
+        a.flags = f;
+        ZK_TRY(launch_pass(a, stream));
+    }
+    if (plan.np > 1) {
+        const u64 n = 1ull << L;
+        const u64 blocks = (n / 2 + 255) / 256;
+        const u32 grid = (u32)(blocks < (u64)num_sms() * 16 ? blocks : (u64)num_sms() * 16);
+        bitrev_kernel<<<grid, 256, 0, stream>>>(v, L, n);
+        ZK_TRY(cudaGetLastError());
+    }
+    return cudaSuccess;
+}
+
+}  // namespace ntt
+}  // namespace zk
+
+using namespace zk;
+
+extern "C" cudaError_t ssip_ntt(PolyPtr x, const unsigned int *twiddle, unsigned int log_len, cudaStream_t stream,
+                                const unsigned int, const unsigned int) {
+    if (log_len == 0) return cudaSuccess;
+    ZK_CHECK_ARG(log_len <= 28 && twiddle != nullptr);
+    ZK_CHECK_ARG(x.len == (1ull << log_len));
+    View v;
+    ZK_CHECK_ARG(make_view(x, &v));
+    return ntt::run(v, nullptr, 0, log_len, twiddle, nullptr, nullptr, nullptr, stream);
+}
+
+extern "C" cudaError_t zkp_ntt_ex(PolyPtr x, const unsigned int *twiddle, unsigned int log_len,
+                                  const unsigned int *shift_d, const unsigned int *scale_d, cudaStream_t stream) {
+    ZK_CHECK_ARG(log_len <= 28 && twiddle != nullptr);
+    ZK_CHECK_ARG(x.len == (1ull << log_len));
+    View v;
+    ZK_CHECK_ARG(make_view(x, &v));
+    if (log_len == 0) {
+        // a length-1 transform is the identity, but shift^0 = 1 and the scale still apply
+        if (!scale_d) return cudaSuccess;
+        return distribute_powers(x, scale_d, 1, stream);
+    }
+    return ntt::run(v, nullptr, 0, log_len, twiddle, nullptr, shift_d, scale_d, stream);
+}
+
+extern "C" cudaError_t zkp_coset_lde(PolyPtr out, ConstPolyPtr in, const unsigned int *twiddle, unsigned int log_in,
+                                     unsigned int log_out, const unsigned int *shift_d, cudaStream_t stream) {
+    ZK_CHECK_ARG(log_out <= 28 && log_in <= log_out && log_out >= 1 && twiddle != nullptr);
+    ZK_CHECK_ARG(out.len == (1ull << log_out) && in.len == (1ull << log_in));
+    View vo, vi;
+    ZK_CHECK_ARG(make_view(out, &vo) && make_view(in, &vi));
+    return ntt::run(vo, &vi, in.len, log_out, twiddle, nullptr, shift_d, nullptr, stream);
+}
+
+extern "C" unsigned int zkp_ntt_num_passes(unsigned int log_len) {
+    ntt::Plan p = ntt::make_plan(log_len);
+    return p.np + (p.np > 1 ? 1 : 0);
+}
+
+extern "C" cudaError_t recompute_ntt(PolyPtr x, const unsigned int *pq_d, unsigned int pq_deg,
+                                     const unsigned int *omegas_d, unsigned int log_len, cudaStream_t stream,
+                                     const unsigned int, const unsigned int) {
+    (void)pq_d;
+    (void)pq_deg;
+    if (log_len == 0) return cudaSuccess;
+    ZK_CHECK_ARG(log_len <= 28 && omegas_d != nullptr);
+    ZK_CHECK_ARG(x.len == (1ull << log_len));
+    View v;
+    ZK_CHECK_ARG(make_view(x, &v));
+    return ntt::run(v, nullptr, 0, log_len, nullptr, omegas_d, nullptr, nullptr, stream);
+}
+
+extern "C" cudaError_t distribute_powers(PolyPtr poly, const unsigned int *powers, unsigned long long power_num,
+                                         cudaStream_t stream) {
+    View v;
+    ZK_CHECK_ARG(make_view(poly, &v));
+    if (v.len == 0) return cudaSuccess;
+    ZK_CHECK_ARG(powers != nullptr && power_num > 0);
+    const u64 blocks = (v.len + 255) / 256;
+    const u32 grid = (u32)(blocks < (u64)num_sms() * 32 ? blocks : (u64)num_sms() * 32);
+    ntt::distribute_powers_kernel<<<grid, 256, 0, stream>>>(v, powers, power_num, v.len);
+    return cudaGetLastError();
+}
+
+extern "C" cudaError_t ssip_precompute(unsigned int *twiddle, unsigned int len, const unsigned int *unit) {
+    if (len == 0) return cudaSuccess;
+    ZK_CHECK_ARG(twiddle != nullptr && unit != nullptr);
+    // roots are generated on the device and copied to the caller's host table
+    u32 *d_out = nullptr, *d_unit = nullptr;
+    ZK_TRY(cudaMalloc(&d_out, (size_t)len * 32));
+    cudaError_t err = cudaMalloc(&d_unit, 32);
+    if (err == cudaSuccess) err = cudaMemcpy(d_unit, unit, 32, cudaMemcpyHostToDevice);
+    if (err == cudaSuccess) {
+        const u64 threads = ((u64)len + 63) / 64;
+        ntt::powers_kernel<<<(u32)((threads + 255) / 256), 256>>>(d_out, d_unit, len);
+        err = cudaGetLastError();
+    }
+    if (err == cudaSuccess) err = cudaMemcpy(twiddle, d_out, (size_t)len * 32, cudaMemcpyDeviceToHost);
+    cudaFree(d_out);
+    if (d_unit) cudaFree(d_unit);
+    return err;
+}
+
+extern "C" void gen_pq_omegas(unsigned int *pq, unsigned int *omegas, unsigned int pq_deg, unsigned int len,
+                              unsigned int *unit) {
+    // precompute.cuh:89-113, byte for byte
+    const zkh::Params &P = zkh::fr();
+    const zkh::Fe u = zkh::load(unit);
+    const size_t pq_len = (size_t)(1u << pq_deg >> 1);
+    memset(pq, 0, pq_len * 32);
+    zkh::store(pq, zkh::one(P));
+    zkh::Fe tw = zkh::pow(P, u, (uint64_t)(len >> pq_deg));
+    if (pq_deg > 1) {
+        zkh::store(pq + 8, tw);
+        zkh::Fe last = tw;
+        for (size_t i = 2; i < pq_len; i++) {
+            last = zkh::mul(P, last, tw);
+            zkh::store(pq + i * 8, last);
+        }
+    }
+    zkh::store(omegas, u);
+    zkh::Fe last = u;
+    for (int i = 1; i < 32; i++) {
+        last = zkh::mul(P, last, last);
+        zkh::store(omegas + i * 8, last);
+    }
+}

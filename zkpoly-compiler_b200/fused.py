@@ -1,0 +1,257 @@
+"""Fused elementwise kernels: host-side mirror of the reference's FusedOp code generator
+(core/src/fused_kernels/kernel_gen.rs:47-617) and FusedKernel runtime wrapper
+(core/src/fused_kernels.rs:76-196).
+
+A FusedGraph is the reference's ArithGraph restated as a topologically ordered node list:
+  ("input",  name, kind, side, index)   kind in {"poly", "scalar", "periodic"};
+                                        side "var" (ConstPolyPtr) or "mut" (PolyPtr)
+  (op, name, lhs, rhs)                  op in {"add", "sub", "mul"}: Pp / Ss / Sp products
+  ("sp_add"|"sp_sub"|"sp_subby", name, scalar, poly)   scalar-poly add/sub; on a Coef graph
+                                        they touch index 0 of the first chunk only
+                                        (kernel_gen.rs:501-545)
+  ("neg", name, x) / ("pow", name, x, exponent)
+  ("output", mut_index, src)
+"periodic" is an addition: input element i is read at i mod len (the 8 distinct values of
+1/Z_H on an 8x coset are such an input).  Division and inversion are not fused, as in the
+reference (batched_invert handles them).
+
+The generated CUDA exports `cudaError_t <name>(ConstPolyPtr const* vars, PolyPtr const*
+mut_vars, unsigned long long len, bool is_first, void* local_buffer, cudaStream_t)` - the
+signature the reference's runtime calls (kernel_gen.rs:286-307) - and is compiled for sm_100a
+into lib<name>.so.  Register allocation is left to ptxas; the local (spill) buffer argument is
+accepted and unused, so get_temp_buffer_size() is 0.
+"""
+from __future__ import annotations
+
+import ctypes
+import hashlib
+import os
+import subprocess
+from dataclasses import dataclass, field
+
+import torch
+
+from .native import PolyPtr, check
+from .scalar import ScalarArray, require_cuda, stream_handle
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+FUSED_DIR = os.path.join(HERE, "lib", "fused")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+
+_BIN = {"add": "Fr::add", "sub": "Fr::sub", "mul": "Fr::mul"}
+
+
+@dataclass
+class FusedGraph:
+    nodes: list
+    coef: bool = False          # poly_repr == Coef (kernel_gen.rs:501-545)
+    num_vars: int = field(init=False, default=0)
+    num_mut_vars: int = field(init=False, default=0)
+
+    def __post_init__(self):
+        nv = nm = 0
+        for n in self.nodes:
+            if n[0] == "input":
+                if n[3] == "var":
+                    nv = max(nv, n[4] + 1)
+                else:
+                    nm = max(nm, n[4] + 1)
+            elif n[0] == "output":
+                nm = max(nm, n[1] + 1)
+        self.num_vars, self.num_mut_vars = nv, nm
+
+    def key(self) -> str:
+        return hashlib.sha1(repr((self.nodes, self.coef)).encode()).hexdigest()[:16]
+
+
+class FusedOp:
+    """Generates and builds one fused kernel (kernel_gen.rs FusedOp::new / gen)."""
+
+    def __init__(self, graph: FusedGraph, name: str | None = None):
+        self.graph = graph
+        self.name = name or f"fused_arith_{graph.key()}"
+
+    def get_temp_buffer_size(self) -> int:
+        return 0
+
+    def gen_source(self) -> str:
+        g = self.graph
+        kinds = {}
+        pre, body = [], []
+        for n in g.nodes:
+            op = n[0]
+            if op == "input":
+                _, name, kind, side, idx = n
+                arr = "sv" if side == "var" else "smv"
+                kinds[name] = kind
+                if kind == "scalar":
+                    pre.append(f"    const Fr {name} = Fr::load({arr}[{idx}].base);")
+                elif kind == "periodic":
+                    body.append(f"        const Fr {name} = Fr::load(fused::periodic_at({arr}[{idx}], idx));")
+                else:
+                    body.append(f"        const Fr {name} = Fr::load({arr}[{idx}].at(idx));")
+            elif op in _BIN:
+                _, name, lhs, rhs = n
+                body.append(f"        const Fr {name} = {_BIN[op]}({lhs}, {rhs});")
+                kinds[name] = "scalar" if kinds[lhs] == kinds[rhs] == "scalar" else "poly"
+            elif op in ("sp_add", "sp_sub", "sp_subby"):
+                _, name, s, p = n
+                full = {"sp_add": f"Fr::add({s}, {p})", "sp_sub": f"Fr::sub({s}, {p})",
+                        "sp_subby": f"Fr::sub({p}, {s})"}[op]
+                if g.coef:
+                    rest = {"sp_add": p, "sp_sub": f"Fr::neg({p})", "sp_subby": p}[op]
+                    body.append(f"        const Fr {name} = (idx == 0 && is_first) ? {full} : {rest};")
+                else:
+                    body.append(f"        const Fr {name} = {full};")
+                kinds[name] = "poly"
+            elif op == "neg":
+                _, name, x = n
+                body.append(f"        const Fr {name} = Fr::neg({x});")
+                kinds[name] = kinds[x]
+            elif op == "pow":
+                _, name, x, e = n
+                body.append(f"        const Fr {name} = Fr::pow_u64({x}, {int(e)}ull);")
+                kinds[name] = kinds[x]
+            elif op == "output":
+                _, idx, src = n
+                if kinds.get(src) == "scalar":
+                    body.append(f"        if (idx == 0) {src}.canonical().store(smv[{idx}].base);")
+                else:
+                    body.append(f"        {src}.canonical().store(smv[{idx}].at(idx));")
+            else:
+                raise ValueError(f"unsupported fused op {op}")
+        nv, nm = max(g.num_vars, 1), max(g.num_mut_vars, 1)
+        inc = os.path.join(CSRC, "fused_rt.cuh")
+        return f"""// generated by zkpoly-compiler_b200/fused.py for graph {g.key()}
+#include "{inc}"
+using namespace zk;
+
+__global__ void __launch_bounds__(256) {self.name}_kernel(const ConstPolyPtr *vars, const PolyPtr *mut_vars,
+                                                        unsigned long long len, bool is_first) {{
+    __shared__ View sv[{nv}];
+    __shared__ View smv[{nm}];
+    if (threadIdx.x < {g.num_vars}) sv[threadIdx.x] = fused::device_view(vars[threadIdx.x]);
+    if (threadIdx.x < {g.num_mut_vars}) smv[threadIdx.x] = fused::device_view(mut_vars[threadIdx.x]);
+    __syncthreads();
+{chr(10).join(pre)}
+    const u64 stride = (u64)gridDim.x * blockDim.x;
+    for (u64 idx = (u64)blockIdx.x * blockDim.x + threadIdx.x; idx < len; idx += stride) {{
+{chr(10).join(body)}
+    }}
+}}
+
+extern "C" cudaError_t {self.name}(ConstPolyPtr const *vars, PolyPtr const *mut_vars, unsigned long long len,
+                                   bool is_first, void *local_buffer, cudaStream_t stream) {{
+    (void)local_buffer;
+    if (len == 0) return cudaSuccess;
+    if (vars == nullptr && {g.num_vars} > 0) return cudaErrorInvalidValue;
+    if (mut_vars == nullptr) return cudaErrorInvalidValue;
+    {self.name}_kernel<<<fused::fused_grid(len, 256), 256, 0, stream>>>(vars, mut_vars, len, is_first);
+    return cudaGetLastError();
+}}
+"""
+
+    def lib_path(self) -> str:
+        return os.path.join(FUSED_DIR, f"lib{self.name}.so")
+
+    def gen(self, target_dir: str = FUSED_DIR) -> str:
+        os.makedirs(target_dir, exist_ok=True)
+        src = os.path.join(target_dir, f"{self.name}.cu")
+        text = self.gen_source()
+        if not os.path.exists(src) or open(src).read() != text:
+            with open(src, "w") as f:
+                f.write(text)
+        return src
+
+    def build(self, force: bool = False) -> str:
+        src = self.gen()
+        out = self.lib_path()
+        deps = [src, os.path.join(CSRC, "fused_rt.cuh"), os.path.join(CSRC, "field.cuh"),
+                os.path.join(CSRC, "common.cuh")]
+        if force or not os.path.exists(out) or any(os.path.getmtime(d) > os.path.getmtime(out) for d in deps):
+            cmd = [NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
+                   "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC", "-shared", "-o", out + ".tmp", src]
+            res = subprocess.run(cmd, capture_output=True, text=True)
+            if res.returncode != 0:
+                raise RuntimeError(f"nvcc failed for fused kernel {self.name}:\n{res.stderr}")
+            os.replace(out + ".tmp", out)
+        return out
+
+
+_loaded: dict[str, ctypes.CDLL] = {}
+
+
+class FusedKernel:
+    """core/src/fused_kernels.rs:76-196: loads the built kernel and calls it with the PolyPtr
+    arrays copied into a device argument buffer."""
+
+    def __init__(self, op: FusedOp):
+        require_cuda()
+        self.op = op
+        path = op.build()
+        if path not in _loaded:
+            _loaded[path] = ctypes.CDLL(path)
+        fn = getattr(_loaded[path], op.name)
+        fn.restype = ctypes.c_int
+        fn.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_ulonglong, ctypes.c_bool, ctypes.c_void_p,
+                       ctypes.c_void_p]
+        self.fn = fn
+        g = op.graph
+        self.arg_buffer = torch.empty(max(g.num_vars + g.num_mut_vars, 1) * ctypes.sizeof(PolyPtr),
+                                      dtype=torch.uint8, device="cuda")
+
+    def __call__(self, mut_vars: list, vars_: list, stream=None, is_first: bool = True):
+        """mut_vars / vars_: ScalarArray (polys) or (1, 8) int32 device tensors (scalars).
+        The element count is the length of the polynomial arguments (fused_kernels.rs:110-160)."""
+        g = self.op.graph
+        length = 0
+        ptrs = []
+        for v in list(vars_) + list(mut_vars):
+            if isinstance(v, ScalarArray):
+                ptrs.append(v.poly_ptr())
+            else:
+                ptrs.append(PolyPtr(v.data_ptr(), 1, 0, 0, 1))
+        periodic = {n[4] for n in g.nodes if n[0] == "input" and n[2] == "periodic" and n[3] == "var"}
+        for i, v in enumerate(list(vars_) + list(mut_vars)):
+            if isinstance(v, ScalarArray) and not (i < len(vars_) and i in periodic):
+                if length in (0, 1):
+                    length = v.len
+                else:
+                    assert length == v.len, "fused kernel operands differ in length"
+        length = max(length, 1)
+        arr = (PolyPtr * len(ptrs))(*ptrs)
+        host = torch.frombuffer(bytearray(bytes(arr)), dtype=torch.uint8)
+        self.arg_buffer[: host.numel()].copy_(host, non_blocking=False)
+        base = self.arg_buffer.data_ptr()
+        check(self.fn(base, base + len(vars_) * ctypes.sizeof(PolyPtr), length, is_first, None,
+                      stream_handle(stream)), self.op.name)
+
+
+# ------------------------------------------------------------------ graphs used by the path
+def quotient_graph() -> FusedGraph:
+    """(a*b - c - z*z(wX)) * zh_inv[i mod 8] on the 8x extended coset: the quotient numerator
+    of the fused-pipeline workload divided by the vanishing polynomial."""
+    return FusedGraph([
+        ("input", "a", "poly", "var", 0),
+        ("input", "b", "poly", "var", 1),
+        ("input", "c", "poly", "var", 2),
+        ("input", "z", "poly", "var", 3),
+        ("input", "zw", "poly", "var", 4),
+        ("input", "zh", "periodic", "var", 5),
+        ("mul", "ab", "a", "b"),
+        ("sub", "t0", "ab", "c"),
+        ("mul", "zz", "z", "zw"),
+        ("sub", "t1", "t0", "zz"),
+        ("mul", "q", "t1", "zh"),
+        ("output", 0, "q"),
+    ])
+
+
+def quotient_kernel() -> FusedKernel:
+    return FusedKernel(FusedOp(quotient_graph(), "zkp_quotient_z8"))
+
+
+def build_path_kernels() -> list[str]:
+    """Builds the fused kernels the hot path uses (called by the package build)."""
+    return [FusedOp(quotient_graph(), "zkp_quotient_z8").build()]

@@ -1,0 +1,106 @@
+"""Loads the in-tree CUDA libraries (lib/*.so) through ctypes and declares their C ABI.
+
+There is no CPU fallback: every entry point of this package calls into these libraries, and
+loading fails loudly when a library is missing or no CUDA device is present.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_DIR = os.path.join(HERE, "lib")
+
+c_u32p = ctypes.POINTER(ctypes.c_uint32)
+c_void_p = ctypes.c_void_p
+cudaError_t = ctypes.c_int
+
+
+class PolyPtr(ctypes.Structure):
+    """core/src/common/iter/src/iter.cuh:12-18 / core/src/poly_ptr.rs:4-11"""
+    _fields_ = [("ptr", ctypes.c_void_p), ("len", ctypes.c_size_t), ("rotate", ctypes.c_size_t),
+                ("offset", ctypes.c_size_t), ("whole_len", ctypes.c_size_t)]
+
+
+ConstPolyPtr = PolyPtr  # identical layout (iter.cuh:20-26)
+
+_libs: dict[str, ctypes.CDLL] = {}
+
+# symbol -> (restype, argtypes)
+SIGNATURES = {
+    "libntt.so": {
+        "ssip_ntt": (cudaError_t, [PolyPtr, c_void_p, ctypes.c_uint, c_void_p, ctypes.c_uint, ctypes.c_uint]),
+        "ssip_precompute": (cudaError_t, [c_void_p, ctypes.c_uint, c_void_p]),
+        "recompute_ntt": (cudaError_t, [PolyPtr, c_void_p, ctypes.c_uint, c_void_p, ctypes.c_uint, c_void_p,
+                                        ctypes.c_uint, ctypes.c_uint]),
+        "gen_pq_omegas": (None, [c_void_p, c_void_p, ctypes.c_uint, ctypes.c_uint, c_void_p]),
+        "distribute_powers": (cudaError_t, [PolyPtr, c_void_p, ctypes.c_ulonglong, c_void_p]),
+        "zkp_ntt_ex": (cudaError_t, [PolyPtr, c_void_p, ctypes.c_uint, c_void_p, c_void_p, c_void_p]),
+        "zkp_coset_lde": (cudaError_t, [PolyPtr, PolyPtr, c_void_p, ctypes.c_uint, ctypes.c_uint, c_void_p,
+                                        c_void_p]),
+        "zkp_ntt_num_passes": (ctypes.c_uint, [ctypes.c_uint]),
+    },
+    "libmsm.so": {
+        "msm": (cudaError_t, [ctypes.POINTER(c_void_p), ctypes.POINTER(ctypes.c_ulong), ctypes.c_ulonglong,
+                              ctypes.c_uint, ctypes.c_uint, ctypes.c_uint, ctypes.c_uint, ctypes.c_uint,
+                              ctypes.POINTER(ctypes.c_uint), ctypes.POINTER(c_void_p), ctypes.c_uint,
+                              ctypes.POINTER(c_void_p), ctypes.POINTER(c_void_p)]),
+        "msm_precompute": (cudaError_t, [ctypes.c_ulonglong, ctypes.POINTER(c_void_p), ctypes.c_uint]),
+        "zkp_msm_workspace_size": (ctypes.c_ulonglong, [ctypes.c_ulonglong, ctypes.c_uint, ctypes.c_uint]),
+        "zkp_msm_default_window": (ctypes.c_uint, [ctypes.c_ulonglong]),
+        "zkp_msm_device": (cudaError_t, [c_void_p, ctypes.c_ulonglong, c_void_p, ctypes.c_uint, c_void_p,
+                                         ctypes.c_ulonglong, ctypes.c_uint, c_void_p, c_void_p]),
+        "zkp_msm_precompute_device": (cudaError_t, [c_void_p, ctypes.c_ulonglong, ctypes.c_uint, ctypes.c_uint,
+                                                    c_void_p]),
+    },
+    "libpoly.so": {
+        "poly_add": (cudaError_t, [PolyPtr, PolyPtr, PolyPtr, c_void_p]),
+        "poly_sub": (cudaError_t, [PolyPtr, PolyPtr, PolyPtr, c_void_p]),
+        "poly_mul": (cudaError_t, [PolyPtr, PolyPtr, PolyPtr, c_void_p]),
+        "poly_one_lagrange": (cudaError_t, [PolyPtr, c_void_p]),
+        "poly_one_coef": (cudaError_t, [PolyPtr, c_void_p]),
+        "poly_zero": (cudaError_t, [PolyPtr, c_void_p]),
+        "poly_eval": (cudaError_t, [c_void_p, ctypes.POINTER(ctypes.c_ulong), PolyPtr, c_void_p, c_void_p, c_void_p]),
+        "kate_division": (cudaError_t, [c_void_p, ctypes.POINTER(ctypes.c_ulong), ctypes.c_uint, PolyPtr, c_void_p,
+                                        PolyPtr, c_void_p]),
+        "scan_mul": (cudaError_t, [c_void_p, ctypes.POINTER(ctypes.c_ulong), PolyPtr, c_void_p]),
+        "batched_invert": (cudaError_t, [c_void_p, ctypes.POINTER(ctypes.c_ulong), PolyPtr, c_void_p]),
+        "inv_scalar": (cudaError_t, [c_void_p, c_void_p]),
+        "scalar_pow": (cudaError_t, [c_void_p, ctypes.c_ulonglong, c_void_p]),
+    },
+}
+
+
+class CudaError(RuntimeError):
+    def __init__(self, code: int, where: str):
+        super().__init__(f"{where} returned cudaError_t {code}")
+        self.code = code
+
+
+def lib_path(name: str) -> str:
+    return os.path.join(LIB_DIR, name)
+
+
+def load(name: str) -> ctypes.CDLL:
+    """dlopen lib/<name> and declare its symbols; raises if the library was not built."""
+    if name in _libs:
+        return _libs[name]
+    path = lib_path(name)
+    if not os.path.exists(path):
+        raise RuntimeError(f"CUDA library {path} is missing: run __graft_entry__.build() first")
+    lib = ctypes.CDLL(path)
+    for sym, (res, args) in SIGNATURES.get(name, {}).items():
+        fn = getattr(lib, sym)
+        fn.restype = res
+        fn.argtypes = args
+    _libs[name] = lib
+    return lib
+
+
+def check(code: int, where: str) -> None:
+    if code != 0:
+        raise CudaError(code, where)
+
+
+def loaded_paths():
+    return {n: lib_path(n) for n in _libs}
