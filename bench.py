@@ -1,0 +1,373 @@
+"""Benchmark: MSM points/s at n = 2^22 and NTT elems/s at n = 2^24 over BN254 on B200.
+
+One step = one forward NTT of 2^24 Fr elements followed by one MSM of 2^22 G1 points, inputs
+resident in HBM (both larger than L2, so nothing is served from cache between steps).  The
+JSON line's `value` is the MSM throughput (points/s); the NTT throughput is under "ntt".
+`e2e` repeats both through the reference-facing C ABI (msm() with host tables; ssip_ntt with a
+host->device copy in and a device->host copy out) from pinned host memory.
+
+`--impl reference` times the reference's CPU path instead: halo2 best_multiexp / best_fft as
+restated by the oracle, on all host cores, on a bounded sample of the same workload.
+
+Multi-GPU: one process per GPU (torchrun); every rank runs its own replica of the step
+("replicas only": the path has no exchange step), timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "MSM points/s (2^22) & NTT elems/s (2^24); served p50/p99 vs plain per-call"
+MSM_LOG, NTT_LOG = 22, 24
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (SM clock, throttle reasons)."""
+
+    def __init__(self, index: int):
+        self.index, self.rows, self.proc = index, [], None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) == 7:
+                self.rows.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.3)
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[3 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+# ------------------------------------------------------------------ CPU (reference path)
+def cpu_reference(sample_msm_log=16, sample_ntt_log=20, reps=1):
+    """halo2 best_multiexp / best_fft restated (oracle), all host threads, bounded samples."""
+    from oracle import oracle as orc
+    orc.build()
+    th = orc.threads()
+    s = orc.gen_fr(1, 1 << sample_msm_log)
+    p = orc.gen_points(2, 1 << sample_msm_log)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        orc.best_multiexp(s, p)
+    msm_t = (time.perf_counter() - t0) / reps
+    a = orc.gen_fr(0, 1 << sample_ntt_log)
+    w = orc.root_of_unity(sample_ntt_log)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        orc.best_fft(a, w, sample_ntt_log)
+    ntt_t = (time.perf_counter() - t0) / reps
+    return {
+        "msm_points_per_s": (1 << sample_msm_log) / msm_t,
+        "ntt_elems_per_s": (1 << sample_ntt_log) / ntt_t,
+        "cores": th,
+        "msm_sample": f"best_multiexp n=2^{sample_msm_log} (seeds 1/2), {msm_t:.2f} s",
+        "ntt_sample": f"best_fft n=2^{sample_ntt_log} (seed 0), {ntt_t:.2f} s",
+    }
+
+
+def run_reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    steps = []
+    for _ in range(args.warmup):
+        cpu_reference(args.ref_msm_log, args.ref_ntt_log)
+    for _ in range(args.steps):
+        steps.append(cpu_reference(args.ref_msm_log, args.ref_ntt_log))
+    v = statistics.median([s["msm_points_per_s"] for s in steps])
+    ntt_v = statistics.median([s["ntt_elems_per_s"] for s in steps])
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "points/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32 (BN254 Montgomery limbs)", "data": "synthetic (seeded)",
+        "config": {"workload": f"MSM n=2^{MSM_LOG} + NTT n=2^{NTT_LOG} (BN254), CPU sample "
+                               f"MSM 2^{args.ref_msm_log} / NTT 2^{args.ref_ntt_log}",
+                   "cpu": cpu_model()},
+        "ntt": {"metric": f"NTT elems/s (2^{NTT_LOG})", "value": ntt_v, "unit": "elems/s"},
+        "cpu_baseline": {"value": v, "unit": "points/s", "cores": steps[-1]["cores"], "kind": "port",
+                         "sample": steps[-1]["msm_sample"] + "; " + steps[-1]["ntt_sample"]},
+        "e2e": {"value": v, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ GPU arm
+def run_gpu(args):
+    import numpy as np
+    import torch
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    zk = importlib.import_module("zkpoly-compiler_b200")
+    native, gen = zk.native, importlib.import_module("zkpoly-compiler_b200.gen")
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(dev)
+    n_msm, n_ntt = 1 << MSM_LOG, 1 << NTT_LOG
+
+    with torch.cuda.stream(stream):
+        # inputs generated on the device by the same counter-based generator as the oracle
+        scalars = gen.fr(1, n_msm, dev)
+        points = gen.points(2, n_msm, dev)
+        ntt_in = gen.fr(0, n_ntt, dev)
+        x = zk.ScalarArray(ntt_in.clone())
+        tw = zk.ntt.twiddle_table(NTT_LOG)
+        bases = zk.msm.ResidentBases(points, window=args.window)
+        ws = bases.workspace()
+        res = torch.zeros(16, dtype=torch.int32, device=dev)
+    torch.cuda.synchronize()
+
+    def ntt_step():
+        zk.ntt.ssip_ntt(x, tw, stream)
+
+    def msm_step():
+        bases.msm(scalars, res, ws, stream)
+
+    # ---- warm-up, then the timed region: K steps between barriers + syncs
+    for _ in range(args.warmup):
+        ntt_step()
+        msm_step()
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    ntt_ms, msm_ms = 0.0, 0.0
+    if world > 1:
+        torch.distributed.barrier()
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        for _ in range(args.steps):
+            ntt_step()
+        ev[1].record(stream)
+        for _ in range(args.steps):
+            msm_step()
+        ev[2].record(stream)
+        torch.cuda.synchronize()
+    ntt_ms = ev[0].elapsed_time(ev[1]) / args.steps
+    msm_ms = ev[1].elapsed_time(ev[2]) / args.steps
+    step_ms = ntt_ms + msm_ms
+    if world > 1:
+        t = torch.tensor([ntt_ms, msm_ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ntt_ms, msm_ms = t.tolist()
+        step_ms = ntt_ms + msm_ms
+
+    # ---- per-kernel timing from the libraries' own stream events (separate, untimed runs)
+    native.profile_enable("libntt.so", True)
+    pass_ms = []
+    for _ in range(3):
+        ntt_step()
+        prof = native.profile_read("libntt.so")
+        pass_ms += [ms for name, ms in prof if name == "ntt_pass"]
+        bitrev_ms = [ms for name, ms in prof if name == "bitrev"]
+    native.profile_enable("libntt.so", False)
+    native.profile_enable("libmsm.so", True)
+    stages = {}
+    for _ in range(3):
+        msm_step()
+        for name, ms in native.profile_read("libmsm.so"):
+            stages.setdefault(name, []).append(ms)
+    native.profile_enable("libmsm.so", False)
+    stage_ms = {k: statistics.median(v) for k, v in stages.items()}
+
+    # ---- IMAD peak probe (measured on this GPU)
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    probe_out = torch.empty(sms * 8 * 256, dtype=torch.int32, device=dev)
+    lib_msm = native.load("libmsm.so")
+    iters = 4096
+    lib_msm.zkp_imad_probe(sms * 8, iters, probe_out.data_ptr(), stream.cuda_stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(5):
+        lib_msm.zkp_imad_probe(sms * 8, iters, probe_out.data_ptr(), stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    imad_per_s = 5 * sms * 8 * 256 * iters * 16 / (e0.elapsed_time(e1) / 1e3)
+
+    # ---- e2e through the reference C ABI from pinned host memory
+    h_scal = scalars.cpu().pin_memory()
+    h_pts = points.cpu().pin_memory()
+    h_ntt = ntt_in.cpu().pin_memory()
+    h_out = torch.empty_like(h_ntt).pin_memory()
+    import ctypes
+    cfg = zk.msm.MsmConfig(cards=[local])
+    sizes = zk.msm.MSM(cfg).get_buffer_size(n_msm)
+    buf = torch.empty(sizes[0], dtype=torch.uint8, device=dev)
+    ptrs = (ctypes.c_void_p * 1)(buf.data_ptr())
+    cards = (ctypes.c_uint * 1)(local)
+    hp = (ctypes.c_void_p * 1)(h_pts.data_ptr())
+    hs = (ctypes.c_void_p * 1)(h_scal.data_ptr())
+    result = np.zeros(16, dtype=np.uint32)
+    hr = (ctypes.c_void_p * 1)(result.ctypes.data)
+    x_e2e = zk.ScalarArray.alloc(n_ntt, dev)
+
+    def e2e_msm():
+        native.check(lib_msm.msm(ptrs, None, n_msm, 1, 1, 1, 1, 1, cards, hp, 1, hs, hr), "msm")
+
+    def e2e_ntt():
+        x_e2e.values.copy_(h_ntt, non_blocking=True)
+        zk.ntt.ssip_ntt(x_e2e, tw, stream)
+        h_out.copy_(x_e2e.values, non_blocking=True)
+
+    with torch.cuda.stream(stream):
+        for _ in range(max(1, args.warmup // 2)):
+            e2e_msm()
+            e2e_ntt()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            e2e_msm()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        for _ in range(args.steps):
+            e2e_ntt()
+        stream.synchronize()
+        t2 = time.perf_counter()
+    e2e_msm_s = (t1 - t0) / args.steps
+    e2e_ntt_s = (t2 - t1) / args.steps
+
+    # ---- CPU baseline (rank 0 at N=1)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_reference(args.ref_msm_log, args.ref_ntt_log)
+
+    if rank != 0:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
+    hbm_peak, peak_kind = peaks()
+    pass_avg = statistics.median(pass_ms)
+    ntt_bytes_per_pass = 64 * n_ntt  # one read + one write of every element per pass
+    acc_ms = stage_ms.get("accumulate", float("nan"))
+    msm_mults = 160 * n_msm + 2 * (1 << 15) * 16 * 14  # accounted Fq products (c = 16 accounting)
+    imad_per_mult = 264
+    msm_total_ms = sum(stage_ms.values())
+    launches_per_ntt = zk.ntt.num_passes(NTT_LOG)
+    launches_per_msm = 10
+    line = {
+        "metric": METRIC, "value": world * n_msm / (msm_ms / 1e3), "unit": "points/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32 (BN254 Montgomery limbs, exact)",
+        "data": "synthetic (seeded counter-based generator; points k_i*G)",
+        "config": {"workload": f"MSM n=2^{MSM_LOG} (BN254 G1, resident bases, window {bases.window}) + "
+                               f"NTT n=2^{NTT_LOG} (BN254 Fr, natural order)",
+                   "msm_n": n_msm, "ntt_n": n_ntt, "window": bases.window, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (NTT 512 MiB, MSM points 256 MiB + 537 MiB sorted digits)"},
+        "msm": {"metric": f"MSM points/s (2^{MSM_LOG})", "value": world * n_msm / (msm_ms / 1e3),
+                "ms": msm_ms, "stages_ms": stage_ms},
+        "ntt": {"metric": f"NTT elems/s (2^{NTT_LOG})", "value": world * n_ntt / (ntt_ms / 1e3), "unit": "elems/s",
+                "ms": ntt_ms, "pass_ms": pass_avg, "bitrev_ms": statistics.median(bitrev_ms) if bitrev_ms else None,
+                "hbm_frac_whole_ntt": (64 * n_ntt / (ntt_ms / 1e3) / 1e9) / hbm_peak},
+        "roofline": {"kernel": "ntt_pass_kernel (2^12-point sub-transform pass of the 2^24 NTT)", "bound": "hbm",
+                     "achieved": ntt_bytes_per_pass / (pass_avg / 1e3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": ntt_bytes_per_pass / (pass_avg / 1e3) / 1e9 / hbm_peak, "peak_source": peak_kind,
+                     "traffic": None,
+                     "note": "IMAD-bound kernel: HBM fraction reported as asked; see int_roofline"},
+        "int_roofline": {
+            "imad_peak_per_s": imad_per_s, "imad_per_mont_mul": imad_per_mult,
+            "mont_mul_peak_per_s": imad_per_s / imad_per_mult,
+            "msm_accumulate": {"kernel": "accumulate_kernel", "ms": acc_ms,
+                               "fq_mults_per_s": msm_mults / (msm_total_ms / 1e3),
+                               "frac_whole_msm": (msm_mults / (msm_total_ms / 1e3)) / (imad_per_s / imad_per_mult)},
+            "ntt_pass": {"fr_mults_per_pass": (n_ntt // 2) * 12,
+                         "frac": ((n_ntt // 2) * 12 / (pass_avg / 1e3)) / (imad_per_s / imad_per_mult)},
+        },
+        "e2e": {"value": world * n_msm / e2e_msm_s, "unit": "points/s",
+                "h2d_bytes_per_step": n_msm * (64 + 32) + n_ntt * 32, "d2h_bytes_per_step": 64 + n_ntt * 32,
+                "ntt_elems_per_s": world * n_ntt / e2e_ntt_s,
+                "path": "msm(): reference C ABI, host tables in, host result out; ssip_ntt with H2D/D2H"},
+        "gpu_launches": args.steps * (launches_per_ntt + launches_per_msm),
+        "clocks": clocks.summary(),
+    }
+    if cpu:
+        line["cpu_baseline"] = {"value": cpu["msm_points_per_s"], "unit": "points/s", "cores": cpu["cores"],
+                                "kind": "port", "sample": cpu["msm_sample"] + "; " + cpu["ntt_sample"],
+                                "ntt_elems_per_s": cpu["ntt_elems_per_s"], "cpu": cpu_model()}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--window", type=int, default=0)
+    ap.add_argument("--ref-msm-log", type=int, default=16)
+    ap.add_argument("--ref-ntt-log", type=int, default=20)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -57,10 +57,36 @@ cudaError_t zkp_msm_device(void *workspace_d, unsigned long long workspace_bytes
                            unsigned int n_tables, const unsigned int *scalars_d, unsigned long long n,
                            unsigned int window, unsigned int *result_d, cudaStream_t stream);
 
+/* ---- batched form (no counterpart in the reference): up to 32 MSMs of uneven sizes share
+ * every stage launch (one counting sort over all their digits, one load-balanced accumulation
+ * over all their buckets, one reduction, one combine with a thread per MSM).  The task table
+ * travels as a kernel parameter, so zkp_msm_batch allocates nothing, copies nothing from the
+ * host and can be captured into a CUDA graph. */
+typedef struct ZkpMsmTask {
+    const unsigned int *points_d;  /* n_tables tables of n affine points */
+    unsigned int n_tables;         /* 0 = the library's configuration */
+    const unsigned int *scalars_d; /* n Montgomery scalars */
+    unsigned long long n;
+    unsigned int window;           /* 0 = choose */
+    unsigned int *result_d;        /* 64-byte affine result */
+} ZkpMsmTask;
+
+unsigned long long zkp_msm_batch_workspace_size(const ZkpMsmTask *tasks, unsigned int ntasks);
+cudaError_t zkp_msm_batch(const ZkpMsmTask *tasks, unsigned int ntasks, void *workspace_d,
+                          unsigned long long workspace_bytes, cudaStream_t stream);
+
 /* Builds the n_tables - 1 extra tables on the device: tables_d holds n_tables * n affine
  * points and its first table is filled by the caller. */
 cudaError_t zkp_msm_precompute_device(unsigned int *tables_d, unsigned long long n, unsigned int window,
                                       unsigned int n_tables, cudaStream_t stream);
+
+/* Benchmark support: per-stage CUDA-event timing of the last MSM (see zkp_ntt_profile_enable). */
+void zkp_msm_profile_enable(int on);
+int zkp_msm_profile_read(float *ms, const char **names, int max);
+
+/* Integer-multiply throughput probe: blocks x 256 threads x iters x 16 IMAD instructions
+ * (out_d: blocks * 256 words).  Used to measure the IMAD peak the MSM roofline divides by. */
+cudaError_t zkp_imad_probe(unsigned int blocks, unsigned int iters, unsigned int *out_d, cudaStream_t stream);
 
 #ifdef __cplusplus
 }

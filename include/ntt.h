@@ -59,6 +59,31 @@ cudaError_t zkp_coset_lde(PolyPtr out, ConstPolyPtr in, const unsigned int *twid
 /* Number of sub-transform passes + permutation passes the plan for 2^log_len uses. */
 unsigned int zkp_ntt_num_passes(unsigned int log_len);
 
+/* ---- batched form (no counterpart in the reference): many transforms of uneven sizes ----
+ * One task per transform, in place; twiddle is the root table of the task's size (use the
+ * inverse root's table and scale_d = n^-1 for an inverse NTT, shift_d for a coset).  A plan
+ * uploads the task tables once; running it launches one persistent kernel per pass (every
+ * task's pencils share the launch) and one batched permutation, with no allocation or host
+ * copy, so it can be captured into a CUDA graph and replayed. */
+typedef struct ZkpNttTask {
+    PolyPtr x;
+    const unsigned int *twiddle;
+    unsigned int log_len;
+    const unsigned int *shift_d;
+    const unsigned int *scale_d;
+} ZkpNttTask;
+
+typedef struct ZkpNttBatchPlan ZkpNttBatchPlan;
+
+cudaError_t zkp_ntt_batch_plan_create(const ZkpNttTask *tasks, unsigned int ntasks, ZkpNttBatchPlan **plan);
+cudaError_t zkp_ntt_batch_run(const ZkpNttBatchPlan *plan, cudaStream_t stream);
+void zkp_ntt_batch_plan_destroy(ZkpNttBatchPlan *plan);
+
+/* Benchmark support: when enabled, the library records a CUDA event on the call's stream after
+ * each launch of its next calls; read returns the per-launch milliseconds of the last call. */
+void zkp_ntt_profile_enable(int on);
+int zkp_ntt_profile_read(float *ms, const char **names, int max);
+
 #ifdef __cplusplus
 }
 #endif

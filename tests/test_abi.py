@@ -12,6 +12,7 @@ HEADER_LIB = {
     "ntt.h": "libntt.so",
     "msm.h": "libmsm.so",
     "poly.h": "libpoly.so",
+    "zkp_gen.h": "libzkp_gen.so",
 }
 
 

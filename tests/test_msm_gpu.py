@@ -103,3 +103,40 @@ def test_msm_2_22_metric_size(zk, orc):
     s = orc.gen_fr(1, n)
     p = orc.gen_points(2, n)
     assert np.array_equal(zk.msm.msm_host(s, p), orc.best_multiexp(s, p))
+
+
+def test_msm_batch_uneven(zk, orc):
+    """Batched form: MSMs of different sizes and windows (one with tables) in one launch set."""
+    sizes = [1, 5, 300, 4096, 20000, 0, 777]
+    windows = [0, 8, 11, 16, 13, 0, 20]
+    N = max(sizes)
+    base_pts = orc.gen_points(300, N)
+    pts_dev = torch.from_numpy(base_pts.view(np.int32).reshape(N, 16).copy()).cuda()
+    tasks, expect = [], []
+    for i, (n, w) in enumerate(zip(sizes, windows)):
+        s = orc.gen_fr(310 + i, max(n, 1))
+        tasks.append({"points": pts_dev, "scalars": torch.from_numpy(s.view(np.int32).reshape(-1, 8).copy()).cuda(),
+                      "n": n, "window": w, "result": torch.full((16,), 7, dtype=torch.int32, device="cuda")})
+        expect.append(orc.best_multiexp(s[:n], base_pts[:n]) if n else np.zeros(8, dtype=np.uint64))
+    # a task over precomputed tables
+    bt = zk.msm.ResidentBases(base_pts[:3000], window=16, n_tables=4)
+    s = orc.gen_fr(320, 3000)
+    tasks.append({"points": bt.tables, "n_tables": 4, "window": 16, "n": 3000,
+                  "scalars": torch.from_numpy(s.view(np.int32).reshape(-1, 8).copy()).cuda(),
+                  "result": torch.zeros(16, dtype=torch.int32, device="cuda")})
+    expect.append(orc.best_multiexp(s, base_pts[:3000]))
+    batch = zk.msm.MsmBatch(tasks)
+    batch.run()
+    for t, e in zip(tasks, expect):
+        assert np.array_equal(t["result"].cpu().numpy().view(np.uint64), e)
+    # graph capture and replay
+    for t in tasks:
+        t["result"].zero_()
+    s = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        batch.run(s)
+    g.replay()
+    torch.cuda.synchronize()
+    for t, e in zip(tasks, expect):
+        assert np.array_equal(t["result"].cpu().numpy().view(np.uint64), e)

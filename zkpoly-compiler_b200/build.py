@@ -23,6 +23,7 @@ LIBS = {
     "libntt.so": ("ntt.cu", []),
     "libmsm.so": ("msm.cu", ["-ldl"]),
     "libpoly.so": ("poly.cu", []),
+    "libzkp_gen.so": ("gen.cu", []),
 }
 
 

@@ -91,3 +91,55 @@ inline int num_sms() {
 }
 
 }  // namespace zk
+
+namespace zk {
+// Stage timing with CUDA events on the launching stream, for the benchmark harness.  Off by
+// default; when on, a library records an event at each stage boundary of its last call.
+struct StageProfiler {
+    static constexpr int MAX = 32;
+    bool on = false;
+    int n = 0;
+    const char *names[MAX];
+    cudaEvent_t ev[MAX + 1];
+    bool created = false;
+
+    void begin(cudaStream_t s) {
+        if (!on) return;
+        if (!created) {
+            for (int i = 0; i <= MAX; i++) cudaEventCreate(&ev[i]);
+            created = true;
+        }
+        n = 0;
+        cudaEventRecord(ev[0], s);
+    }
+    // closes the stage that started at the previous mark
+    void mark(const char *name, cudaStream_t s) {
+        if (!on || n >= MAX) return;
+        names[n] = name;
+        n++;
+        cudaEventRecord(ev[n], s);
+    }
+    int read(float *ms, const char **out_names, int max) {
+        if (!created || n == 0) return 0;
+        cudaEventSynchronize(ev[n]);
+        int k = n < max ? n : max;
+        for (int i = 0; i < k; i++) {
+            cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]);
+            out_names[i] = names[i];
+        }
+        return k;
+    }
+};
+
+inline StageProfiler &profiler() {
+    static StageProfiler p;
+    return p;
+}
+}  // namespace zk
+
+// per-library profiling entry points (each shared object carries its own profiler)
+#define ZK_DEFINE_PROFILER_API(prefix)                                                               \
+    extern "C" void prefix##_profile_enable(int on) { zk::profiler().on = on != 0; }                 \
+    extern "C" int prefix##_profile_read(float *ms, const char **names, int max) {                   \
+        return zk::profiler().read(ms, names, max);                                                  \
+    }

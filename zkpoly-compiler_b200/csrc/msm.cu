@@ -40,35 +40,55 @@ namespace msm {
 
 constexpr int SCALAR_BITS = 254;
 constexpr u32 EMPTY = 0xffffffffu;
+constexpr u32 MAX_TASKS = 32;
 
-struct Config {
-    u64 n;          // points per table
-    u32 c;          // window bits
-    u32 W;          // logical windows = ceil(254 / c)
-    u32 n_tables;   // precomputed tables (1 = none)
-    u32 Wp;         // physical windows = ceil(W / n_tables)
-    u32 B;          // buckets per window = 2^(c-1)
-    u32 K;          // entries per accumulation chunk
-    u32 L;          // buckets per reduction segment
+// One MSM of a batch.  A single MSM is a batch of one.
+struct Task {
+    const u32 *points;   // n_tables tables of n affine points
+    const u32 *scalars;  // n Montgomery scalars
+    u32 *result;         // 64-byte affine result
+    u64 n;
+    u32 n_tables;
+    u32 c;    // window bits
+    u32 W;    // logical windows = ceil(254 / c)
+    u32 Wp;   // physical windows = ceil(W / n_tables)
+    u32 B;    // buckets per window = 2^(c-1)
+    u32 L;    // buckets per reduction segment
 };
 
-inline Config make_config(u64 n, u32 c, u32 n_tables) {
-    Config cfg{};
-    cfg.n = n;
-    cfg.c = c;
-    cfg.W = (SCALAR_BITS + c - 1) / c;
-    cfg.n_tables = n_tables;
-    cfg.Wp = (cfg.W + n_tables - 1) / n_tables;
-    cfg.B = 1u << (c - 1);
-    cfg.L = cfg.B < 16 ? cfg.B : 16;
-    // chunk so that roughly 4 waves of 384 threads per SM cover the entries
-    const u64 entries = n * cfg.W;
-    const u64 threads = (u64)num_sms() * 384 * 4;
-    u64 k = (entries + threads - 1) / threads;
-    if (k < 8) k = 8;
-    if (k > 4096) k = 4096;
-    cfg.K = (u32)k;
-    return cfg;
+// The whole batch travels as a kernel parameter (no device copy, capturable in a graph).
+// Every global index space is the concatenation of the tasks' spaces; *_first are the
+// exclusive prefixes (entry ntasks is the total).
+struct Batch {
+    u32 ntasks;
+    u32 K;  // entries per accumulation chunk
+    Task task[MAX_TASKS];
+    u64 sc_first[MAX_TASKS + 1];   // scalars
+    u64 key_first[MAX_TASKS + 1];  // buckets (Wp * B per task)
+    u64 seg_first[MAX_TASKS + 1];  // reduction segments (key count / L)
+    u32 win_first[MAX_TASKS + 1];  // physical windows
+};
+
+template <typename T>
+ZK_DI u32 find_task(const T *first, u32 ntasks, T x) {
+    u32 lo = 0, hi = ntasks;  // largest t with first[t] <= x
+    while (hi - lo > 1) {
+        const u32 mid = (lo + hi) >> 1;
+        if (first[mid] <= x) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+inline Task make_task(u64 n, u32 c, u32 n_tables) {
+    Task t{};
+    t.n = n;
+    t.c = c;
+    t.W = (SCALAR_BITS + c - 1) / c;
+    t.n_tables = n_tables;
+    t.Wp = (t.W + n_tables - 1) / n_tables;
+    t.B = 1u << (c - 1);
+    t.L = t.B < 16 ? t.B : 16;
+    return t;
 }
 
 // default window width for n points (a cost model in the spirit of
@@ -87,16 +107,37 @@ inline u32 default_window(u64 n) {
     return best;
 }
 
+// fills the prefixes and the chunk size; tasks[] must be set
+inline void finish_batch(Batch &b) {
+    b.sc_first[0] = b.key_first[0] = b.seg_first[0] = 0;
+    b.win_first[0] = 0;
+    u64 entries = 0;
+    for (u32 t = 0; t < b.ntasks; t++) {
+        const Task &k = b.task[t];
+        b.sc_first[t + 1] = b.sc_first[t] + k.n;
+        b.key_first[t + 1] = b.key_first[t] + (u64)k.Wp * k.B;
+        b.seg_first[t + 1] = b.seg_first[t] + (u64)k.Wp * k.B / k.L;
+        b.win_first[t + 1] = b.win_first[t] + k.Wp;
+        entries += k.n * k.W;
+    }
+    // chunk so that roughly 4 waves of 384 threads per SM cover the entries
+    const u64 threads = (u64)num_sms() * 384 * 4;
+    u64 k = (entries + threads - 1) / threads;
+    if (k < 8) k = 8;
+    if (k > 4096) k = 4096;
+    b.K = (u32)k;
+}
+
 // ------------------------------------------------------------------ workspace layout
 struct Layout {
-    size_t points, scalars, counts, cursor, sorted_bucket, sorted_point, bucket_sums, part_pts, part_bucket,
-        part_flag, seg, win, result, total;
-    u64 entries, chunks, segs;
+    size_t counts, cursor, sorted_bucket, sorted_point, bucket_sums, part_pts, part_bucket, part_flag, seg, win,
+        total;
+    u64 nb, entries, chunks, segs, wins;
 };
 
 inline size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
 
-inline Layout make_layout(const Config &cfg, bool with_points, bool with_scalars) {
+inline Layout make_layout(const Batch &b) {
     Layout l{};
     size_t off = 0;
     auto take = [&](size_t bytes) {
@@ -104,23 +145,22 @@ inline Layout make_layout(const Config &cfg, bool with_points, bool with_scalars
         off += align_up(bytes);
         return o;
     };
-    const u64 nb = (u64)cfg.Wp * cfg.B;
-    l.entries = cfg.n * cfg.W;
-    l.chunks = (l.entries + cfg.K - 1) / cfg.K;
-    l.segs = nb / cfg.L;
-    l.points = with_points ? take(cfg.n * cfg.n_tables * 64) : 0;
-    l.scalars = with_scalars ? take(cfg.n * 32) : 0;
-    l.counts = take((nb + 1) * 4);
-    l.cursor = take((nb + 1) * 4);
+    l.nb = b.key_first[b.ntasks];
+    l.entries = 0;
+    for (u32 t = 0; t < b.ntasks; t++) l.entries += b.task[t].n * b.task[t].W;
+    l.chunks = (l.entries + b.K - 1) / b.K;
+    l.segs = b.seg_first[b.ntasks];
+    l.wins = b.win_first[b.ntasks];
+    l.counts = take((l.nb + 1) * 4);
+    l.cursor = take((l.nb + 1) * 4);
     l.sorted_bucket = take(l.entries * 4);
     l.sorted_point = take(l.entries * 4);
-    l.bucket_sums = take(nb * 128);
+    l.bucket_sums = take(l.nb * 128);
     l.part_pts = take(l.chunks * 2 * 128);
     l.part_bucket = take(l.chunks * 2 * 4);
     l.part_flag = take(l.chunks * 2 * 4);
     l.seg = take(l.segs * 128);
-    l.win = take((size_t)cfg.Wp * 128);
-    l.result = take(64);
+    l.win = take(l.wins * 128);
     l.total = off;
     return l;
 }
@@ -149,18 +189,20 @@ ZK_DI void load_digits(Digits &d, const u32 *scalar, u32 c) {
     d.c = c;
 }
 
-// per (scalar, window): bucket key (physical window * B + |d| - 1) and negative flag; key
-// EMPTY for a zero digit
+// per (scalar, window) with a non-zero digit: f(table, local bucket key, negative).  Digits
+// are signed in [-2^(c-1), 2^(c-1)]: a raw window value above 2^(c-1) becomes raw - 2^c with
+// a carry into the next window (signed_digit, msm_impl.cuh:22-33).  254 is not a multiple of
+// c for any c in [2, 24] except 2, so the top window never carries out.
 template <typename F>
-ZK_DI void for_each_digit(const Digits &d, const Config &cfg, F &&f) {
+ZK_DI void for_each_digit(const Digits &d, const Task &k, F &&f) {
     u32 carry = 0;
-    const u32 half = 1u << (cfg.c - 1);
-    for (u32 w = 0; w < cfg.W; w++) {
+    const u32 half = 1u << (k.c - 1);
+    for (u32 w = 0; w < k.W; w++) {
         u32 raw = d.raw(w) + carry;
         bool neg = false;
         u32 mag;
         if (raw > half) {
-            mag = (1u << cfg.c) - raw;
+            mag = (1u << k.c) - raw;
             neg = true;
             carry = 1;
         } else {
@@ -168,31 +210,41 @@ ZK_DI void for_each_digit(const Digits &d, const Config &cfg, F &&f) {
             carry = 0;
         }
         if (mag != 0) {
-            const u32 table = w / cfg.Wp, pw = w % cfg.Wp;
-            f(table, pw * cfg.B + mag - 1, neg);
+            const u32 table = w / k.Wp, pw = w % k.Wp;
+            f(table, pw * k.B + mag - 1, neg);
         }
     }
 }
 
-__global__ void __launch_bounds__(256) count_kernel(const u32 *scalars, Config cfg, u32 *counts) {
+__global__ void __launch_bounds__(256) count_kernel(const Batch b, u32 *counts) {
+    const u64 total = b.sc_first[b.ntasks];
     const u64 stride = (u64)gridDim.x * blockDim.x;
-    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < cfg.n; i += stride) {
+    for (u64 g = (u64)blockIdx.x * blockDim.x + threadIdx.x; g < total; g += stride) {
+        const u32 t = find_task(b.sc_first, b.ntasks, g);
+        const Task &k = b.task[t];
+        const u64 i = g - b.sc_first[t];
         Digits d;
-        load_digits(d, scalars + i * 8, cfg.c);
-        for_each_digit(d, cfg, [&](u32, u32 key, bool) { atomicAdd(counts + key, 1u); });
+        load_digits(d, k.scalars + i * 8, k.c);
+        u32 *cnt = counts + b.key_first[t];
+        for_each_digit(d, k, [&](u32, u32 key, bool) { atomicAdd(cnt + key, 1u); });
     }
 }
 
-__global__ void __launch_bounds__(256) scatter_kernel(const u32 *scalars, Config cfg, u32 *cursor,
-                                                     u32 *sorted_bucket, u32 *sorted_point) {
+__global__ void __launch_bounds__(256) scatter_kernel(const Batch b, u32 *cursor, u32 *sorted_bucket,
+                                                     u32 *sorted_point) {
+    const u64 total = b.sc_first[b.ntasks];
     const u64 stride = (u64)gridDim.x * blockDim.x;
-    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < cfg.n; i += stride) {
+    for (u64 g = (u64)blockIdx.x * blockDim.x + threadIdx.x; g < total; g += stride) {
+        const u32 t = find_task(b.sc_first, b.ntasks, g);
+        const Task &k = b.task[t];
+        const u64 i = g - b.sc_first[t];
+        const u32 kb = (u32)b.key_first[t];
         Digits d;
-        load_digits(d, scalars + i * 8, cfg.c);
-        for_each_digit(d, cfg, [&](u32 table, u32 key, bool neg) {
-            const u32 pos = atomicAdd(cursor + key, 1u);
-            sorted_bucket[pos] = key;
-            sorted_point[pos] = (u32)(table * cfg.n + i) | (neg ? 0x80000000u : 0u);
+        load_digits(d, k.scalars + i * 8, k.c);
+        for_each_digit(d, k, [&](u32 table, u32 key, bool neg) {
+            const u32 pos = atomicAdd(cursor + kb + key, 1u);
+            sorted_bucket[pos] = kb + key;
+            sorted_point[pos] = (u32)(table * k.n + i) | (neg ? 0x80000000u : 0u);
         });
     }
 }
@@ -281,28 +333,31 @@ ZK_DI G1A fetch_point(const u32 *points, u32 code) {
     return p;
 }
 
-// part_flag: 1 = head run (continued from the previous chunk, ends here), 2 = head run that
-// also continues into the next chunk, 3 = tail run (starts here, continues into the next)
-__global__ void __launch_bounds__(256) accumulate_kernel(const u32 *points, const u32 *sorted_bucket,
-                                                        const u32 *sorted_point, const u32 *live, u32 K,
-                                                        u32 *bucket_sums, u32 *part_pts, u32 *part_bucket,
-                                                        u32 *part_flag) {
+// The sorted array (live entries: *live) is cut into chunks of K; one thread per chunk walks
+// it with mixed additions.  A run of one bucket wholly inside the chunk is stored to its
+// bucket; a run cut by a chunk edge leaves a partial: part_flag 1 = head run (continued from
+// the previous chunk, ends here), 2 = head run that also continues into the next chunk,
+// 3 = tail run (starts here, continues into the next).  Buckets of different tasks never
+// share a key, so runs never span two tasks.
+__global__ void __launch_bounds__(256) accumulate_kernel(const Batch b, const u32 *sorted_bucket,
+                                                        const u32 *sorted_point, const u32 *live, u32 *bucket_sums,
+                                                        u32 *part_pts, u32 *part_bucket, u32 *part_flag) {
     const u64 entries = *live;
     const u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x;
-    const u64 start = t * K;
+    const u64 start = t * b.K;
     if (start >= entries) return;
-    const u64 end = start + K < entries ? start + K : entries;
+    const u64 end = start + b.K < entries ? start + b.K : entries;
     const bool from_prev = start > 0 && sorted_bucket[start - 1] == sorted_bucket[start];
     u64 run_start = start;
     u32 cur = sorted_bucket[start];
-    G1X acc = G1X::from_affine(fetch_point(points, sorted_point[start]));
+    const u32 *pts = b.task[find_task(b.key_first, b.ntasks, (u64)cur)].points;
+    G1X acc = G1X::from_affine(fetch_point(pts, sorted_point[start]));
     for (u64 p = start + 1; p <= end; p++) {
-        const u32 b = p < end ? sorted_bucket[p] : EMPTY;
-        if (p < end && b == cur) {
-            acc = g1_madd(acc, fetch_point(points, sorted_point[p]));
+        const u32 bk = p < end ? sorted_bucket[p] : EMPTY;
+        if (p < end && bk == cur) {
+            acc = g1_madd(acc, fetch_point(pts, sorted_point[p]));
             continue;
         }
-        // the run [run_start, p) of bucket `cur` ends here
         const bool head = run_start == start && from_prev;
         const bool to_next = p == end && end < entries && sorted_bucket[end] == cur;
         if (!head && !to_next) {
@@ -314,9 +369,10 @@ __global__ void __launch_bounds__(256) accumulate_kernel(const u32 *points, cons
             part_flag[slot] = head ? (to_next ? 2u : 1u) : 3u;
         }
         if (p < end) {
-            cur = b;
+            cur = bk;
             run_start = p;
-            acc = G1X::from_affine(fetch_point(points, sorted_point[p]));
+            pts = b.task[find_task(b.key_first, b.ntasks, (u64)cur)].points;
+            acc = G1X::from_affine(fetch_point(pts, sorted_point[p]));
         }
     }
 }
@@ -340,52 +396,68 @@ __global__ void __launch_bounds__(256) fixup_kernel(const u32 *live, u32 K, u32 
 }
 
 // ------------------------------------------------------------------ 5: bucket reduction
-// segment g of window w covers buckets b = g*L + 1 .. g*L + L (stored at index b - 1):
-// out = sum_j (g*L + j + 1) * S[g*L + j] = runsum-weighted part + (g*L) * plain sum
-__global__ void __launch_bounds__(128) segment_kernel(const u32 *bucket_sums, u32 B, u32 L, u64 segs, u32 *seg_out) {
+// global segment s of task t covers buckets key_first[t] + s_l*L .. + L - 1; with g the
+// segment's index inside its window, it yields
+//   sum_j (g*L + j + 1) * S_j = (running sums of the segment) + (g*L) * (segment sum)
+__global__ void __launch_bounds__(128) segment_kernel(const Batch b, const u32 *bucket_sums, u32 *seg_out) {
     const u64 s = (u64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= segs) return;
-    const u64 segs_per_window = B / L;
-    const u64 g = s % segs_per_window;
-    const u32 *base = bucket_sums + s * L * 32;
+    if (s >= b.seg_first[b.ntasks]) return;
+    const u32 t = find_task(b.seg_first, b.ntasks, s);
+    const Task &k = b.task[t];
+    const u64 sl = s - b.seg_first[t];
+    const u64 g = sl % (k.B / k.L);
+    const u32 *base = bucket_sums + (b.key_first[t] + sl * k.L) * 32;
     G1X run = G1X::identity(), acc = G1X::identity();
-    for (int j = (int)L - 1; j >= 0; j--) {
+    for (int j = (int)k.L - 1; j >= 0; j--) {
         run = g1_add(run, G1X::load(base + (u64)j * 32));
         acc = g1_add(acc, run);
     }
-    if (g > 0) acc = g1_add(acc, g1_mul_u64(run, g * L));
+    if (g > 0) acc = g1_add(acc, g1_mul_u64(run, g * k.L));
     acc.store(seg_out + s * 32);
 }
 
-// per window: tree-sum of its segments (one CTA per window)
-__global__ void __launch_bounds__(256) window_sum_kernel(const u32 *seg_out, u64 segs_per_window, u32 *win_out) {
+// per physical window (one CTA each): tree-sum of its segments
+__global__ void __launch_bounds__(256) window_sum_kernel(const Batch b, const u32 *seg_out, u32 *win_out) {
     __shared__ u32 sm[256 * 32];
-    const u32 w = blockIdx.x;
-    const u32 *base = seg_out + (u64)w * segs_per_window * 32;
+    const u32 wg = blockIdx.x;
+    const u32 t = find_task(b.win_first, b.ntasks, wg);
+    const Task &k = b.task[t];
+    const u64 spw = k.B / k.L;
+    const u32 *base = seg_out + (b.seg_first[t] + (u64)(wg - b.win_first[t]) * spw) * 32;
     G1X acc = G1X::identity();
-    for (u64 i = threadIdx.x; i < segs_per_window; i += blockDim.x) acc = g1_add(acc, G1X::load(base + i * 32));
+    for (u64 i = threadIdx.x; i < spw; i += blockDim.x) acc = g1_add(acc, G1X::load(base + i * 32));
     acc.store(sm + threadIdx.x * 32);
     __syncthreads();
     for (u32 stride = blockDim.x / 2; stride > 0; stride >>= 1) {
         if (threadIdx.x < stride) {
-            G1X a = G1X::load(sm + threadIdx.x * 32);
-            G1X b = G1X::load(sm + (threadIdx.x + stride) * 32);
-            g1_add(a, b).store(sm + threadIdx.x * 32);
+            G1X x = G1X::load(sm + threadIdx.x * 32);
+            G1X y = G1X::load(sm + (threadIdx.x + stride) * 32);
+            g1_add(x, y).store(sm + threadIdx.x * 32);
         }
         __syncthreads();
     }
-    if (threadIdx.x == 0) G1X::load(sm).store(win_out + (u64)w * 32);
+    if (threadIdx.x == 0) G1X::load(sm).store(win_out + (u64)wg * 32);
 }
 
 // ------------------------------------------------------------------ 6: window combination
-__global__ void combine_kernel(const u32 *win_out, u32 Wp, u32 c, u32 *result) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    G1X acc = G1X::load(win_out + (u64)(Wp - 1) * 32);
-    for (int w = (int)Wp - 2; w >= 0; w--) {
-        for (u32 k = 0; k < c; k++) acc = g1_dbl(acc);
-        acc = g1_add(acc, G1X::load(win_out + (u64)w * 32));
+// one thread per task: Horner over the physical windows (c doublings each), then affine
+__global__ void combine_kernel(const Batch b, const u32 *win_out) {
+    const u32 t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= b.ntasks) return;
+    const Task &k = b.task[t];
+    const u32 *w = win_out + (u64)b.win_first[t] * 32;
+    G1X acc = G1X::load(w + (u64)(k.Wp - 1) * 32);
+    for (int i = (int)k.Wp - 2; i >= 0; i--) {
+        for (u32 d = 0; d < k.c; d++) acc = g1_dbl(acc);
+        acc = g1_add(acc, G1X::load(w + (u64)i * 32));
     }
-    g1_to_affine(acc).store(result);
+    g1_to_affine(acc).store(k.result);
+}
+
+__global__ void zero_results_kernel(const Batch b) {
+    const u32 t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= b.ntasks || b.task[t].n != 0) return;
+    for (int i = 0; i < 16; i++) b.task[t].result[i] = 0;
 }
 
 // ------------------------------------------------------------------ precompute tables
@@ -412,10 +484,9 @@ inline u32 grid_for(u64 items, u32 block, u32 per_sm = 8) {
     return (u32)(b < cap ? (b == 0 ? 1 : b) : cap);
 }
 
-// Runs one MSM with points / scalars already on the device; `ws` holds the layout regions.
-cudaError_t run_device(const Config &cfg, const Layout &l, char *ws, const u32 *d_points, const u32 *d_scalars,
-                       u32 *d_result, cudaStream_t stream) {
-    const u64 nb = (u64)cfg.Wp * cfg.B;
+// Runs a batch of MSMs whose points / scalars are on the device; `ws` holds the layout
+// regions.  Launches only: no allocation, no host copy.
+cudaError_t run_batch(const Batch &b, const Layout &l, char *ws, cudaStream_t stream) {
     u32 *counts = reinterpret_cast<u32 *>(ws + l.counts);
     u32 *cursor = reinterpret_cast<u32 *>(ws + l.cursor);
     u32 *sb = reinterpret_cast<u32 *>(ws + l.sorted_bucket);
@@ -426,35 +497,61 @@ cudaError_t run_device(const Config &cfg, const Layout &l, char *ws, const u32 *
     u32 *pf = reinterpret_cast<u32 *>(ws + l.part_flag);
     u32 *seg = reinterpret_cast<u32 *>(ws + l.seg);
     u32 *win = reinterpret_cast<u32 *>(ws + l.win);
+    const u64 nb = l.nb;
 
+    StageProfiler &prof = profiler();
+    prof.begin(stream);
     ZK_TRY(cudaMemsetAsync(counts, 0, (nb + 1) * 4, stream));
     ZK_TRY(cudaMemsetAsync(bs, 0, nb * 128, stream));
     ZK_TRY(cudaMemsetAsync(pf, 0, l.chunks * 2 * 4, stream));
-    count_kernel<<<grid_for(cfg.n, 256), 256, 0, stream>>>(d_scalars, cfg, counts);
-    ZK_TRY(cudaGetLastError());
+    prof.mark("memset", stream);
+    const u64 scalars = b.sc_first[b.ntasks];
+    if (scalars) {
+        count_kernel<<<grid_for(scalars, 256), 256, 0, stream>>>(b, counts);
+        ZK_TRY(cudaGetLastError());
+    }
+    prof.mark("count", stream);
     // exclusive scan of the nb + 1 counters: cursor[k] = first slot of bucket k, and
     // counts[nb] becomes the number of live (non-zero digit) entries
     const u64 items = nb + 1;
     const u32 nblocks = (u32)((items + SCAN_BLOCK * SCAN_ITEMS - 1) / (SCAN_BLOCK * SCAN_ITEMS));
-    u32 *block_sums = seg;  // the segment buffer is free until the reduction
+    u32 *block_sums = reinterpret_cast<u32 *>(ws + l.part_pts);  // free until accumulation
     scan_reduce_kernel<<<nblocks, SCAN_BLOCK, 0, stream>>>(counts, items, block_sums);
     scan_blocks_kernel<<<1, SCAN_BLOCK, 0, stream>>>(block_sums, nblocks);
     scan_apply_kernel<<<nblocks, SCAN_BLOCK, 0, stream>>>(counts, items, block_sums, cursor, counts);
     ZK_TRY(cudaGetLastError());
-    scatter_kernel<<<grid_for(cfg.n, 256), 256, 0, stream>>>(d_scalars, cfg, cursor, sb, sp);
-    ZK_TRY(cudaGetLastError());
+    prof.mark("scan", stream);
+    if (scalars) {
+        scatter_kernel<<<grid_for(scalars, 256), 256, 0, stream>>>(b, cursor, sb, sp);
+        ZK_TRY(cudaGetLastError());
+    }
+    prof.mark("scatter", stream);
     const u32 *live = counts + nb;
-    accumulate_kernel<<<(u32)((l.chunks + 255) / 256), 256, 0, stream>>>(d_points, sb, sp, live, cfg.K, bs, pp, pb,
-                                                                         pf);
+    if (l.chunks) {
+        accumulate_kernel<<<(u32)((l.chunks + 255) / 256), 256, 0, stream>>>(b, sb, sp, live, bs, pp, pb, pf);
+        ZK_TRY(cudaGetLastError());
+    }
+    prof.mark("accumulate", stream);
+    if (l.chunks) {
+        fixup_kernel<<<(u32)((l.chunks + 255) / 256), 256, 0, stream>>>(live, b.K, bs, pp, pb, pf);
+        ZK_TRY(cudaGetLastError());
+    }
+    prof.mark("fixup", stream);
+    if (l.segs) {
+        segment_kernel<<<(u32)((l.segs + 127) / 128), 128, 0, stream>>>(b, bs, seg);
+        ZK_TRY(cudaGetLastError());
+    }
+    prof.mark("segment", stream);
+    if (l.wins) {
+        window_sum_kernel<<<(u32)l.wins, 256, 0, stream>>>(b, seg, win);
+        ZK_TRY(cudaGetLastError());
+    }
+    prof.mark("window_sum", stream);
+    combine_kernel<<<(b.ntasks + 31) / 32, 32, 0, stream>>>(b, win);
+    zero_results_kernel<<<(b.ntasks + 31) / 32, 32, 0, stream>>>(b);
     ZK_TRY(cudaGetLastError());
-    fixup_kernel<<<(u32)((l.chunks + 255) / 256), 256, 0, stream>>>(live, cfg.K, bs, pp, pb, pf);
-    ZK_TRY(cudaGetLastError());
-    segment_kernel<<<(u32)((l.segs + 127) / 128), 128, 0, stream>>>(bs, cfg.B, cfg.L, l.segs, seg);
-    ZK_TRY(cudaGetLastError());
-    window_sum_kernel<<<cfg.Wp, 256, 0, stream>>>(seg, cfg.B / cfg.L, win);
-    ZK_TRY(cudaGetLastError());
-    combine_kernel<<<1, 32, 0, stream>>>(win, cfg.Wp, cfg.c, d_result);
-    return cudaGetLastError();
+    prof.mark("combine", stream);
+    return cudaSuccess;
 }
 
 // ------------------------------------------------------------------ library configuration
@@ -464,7 +561,7 @@ cudaError_t run_device(const Config &cfg, const Layout &l, char *ws, const u32 *
 // installed under such a name, so a caller passes exactly as many tables as it would to the
 // reference; under any other name there is one table and the window is chosen per call.
 struct LibConfig {
-    u32 window = 0;   // 0 = choose per call
+    u32 window = 0;  // 0 = choose per call
     u32 target_windows = 0;
 };
 
@@ -504,17 +601,57 @@ inline void resolve(u64 n, u32 window, u32 n_tables_hint, u32 *c, u32 *n_tables)
     *n_tables = nt;
 }
 
+inline Batch single(const u32 *points, u32 n_tables, const u32 *scalars, u64 n, u32 c, u32 *result) {
+    Batch b{};
+    b.ntasks = 1;
+    b.task[0] = make_task(n, c, n_tables);
+    b.task[0].points = points;
+    b.task[0].scalars = scalars;
+    b.task[0].result = result;
+    finish_batch(b);
+    return b;
+}
+
 }  // namespace msm
 }  // namespace zk
 
 using namespace zk;
+
+ZK_DEFINE_PROFILER_API(zkp_msm)
+
+// Integer-multiply throughput probe for the roofline denominator: every thread runs `iters`
+// rounds of 8 independent 32-bit multiply-add chains (mad.lo), 16 IMAD per round with the
+// chains' high halves.  out[tid] keeps the chains live.
+__global__ void __launch_bounds__(256) imad_probe_kernel(u32 iters, u32 seed, u32 *out) {
+    u32 a[8], b = seed | 1u;
+#pragma unroll
+    for (int k = 0; k < 8; k++) a[k] = seed + threadIdx.x * 8 + k;
+    for (u32 i = 0; i < iters; i++) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(a[k]) : "r"(b), "r"(a[(k + 1) & 7]));
+            asm volatile("mad.hi.u32 %0, %0, %1, %2;" : "+r"(a[k]) : "r"(b), "r"(a[(k + 3) & 7]));
+        }
+    }
+    u32 s = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) s ^= a[k];
+    out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+// launches the probe: blocks x 256 threads x iters x 16 IMAD instructions
+extern "C" cudaError_t zkp_imad_probe(unsigned int blocks, unsigned int iters, unsigned int *out_d,
+                                      cudaStream_t stream) {
+    imad_probe_kernel<<<blocks, 256, 0, stream>>>(iters, 0x9e3779b9u, out_d);
+    return cudaGetLastError();
+}
 
 extern "C" unsigned int zkp_msm_default_window(unsigned long long n) { return msm::default_window(n); }
 
 extern "C" unsigned long long zkp_msm_workspace_size(unsigned long long n, unsigned int window, unsigned int n_tables) {
     u32 c, nt;
     msm::resolve(n, window, n_tables, &c, &nt);
-    return msm::make_layout(msm::make_config(n, c, nt), false, false).total;
+    return msm::make_layout(msm::single(nullptr, nt, nullptr, n, c, nullptr)).total;
 }
 
 extern "C" cudaError_t zkp_msm_device(void *workspace_d, unsigned long long workspace_bytes,
@@ -528,10 +665,46 @@ extern "C" cudaError_t zkp_msm_device(void *workspace_d, unsigned long long work
     msm::resolve(n, window, n_tables, &c, &nt);
     ZK_CHECK_ARG(c >= 2 && c <= 24 && nt >= 1);
     ZK_CHECK_ARG(n * nt < (1ull << 31));
-    msm::Config cfg = msm::make_config(n, c, nt);
-    msm::Layout l = msm::make_layout(cfg, false, false);
+    const msm::Batch b = msm::single(points_d, nt, scalars_d, n, c, result_d);
+    const msm::Layout l = msm::make_layout(b);
     ZK_CHECK_ARG(workspace_bytes >= l.total);
-    return msm::run_device(cfg, l, reinterpret_cast<char *>(workspace_d), points_d, scalars_d, result_d, stream);
+    return msm::run_batch(b, l, reinterpret_cast<char *>(workspace_d), stream);
+}
+
+// batches of more than MAX_TASKS are not split here; the caller chunks them
+static cudaError_t build_batch(const ZkpMsmTask *tasks, unsigned int ntasks, msm::Batch *out) {
+    ZK_CHECK_ARG(ntasks >= 1 && ntasks <= msm::MAX_TASKS && tasks != nullptr);
+    msm::Batch b{};
+    b.ntasks = ntasks;
+    for (u32 t = 0; t < ntasks; t++) {
+        const ZkpMsmTask &k = tasks[t];
+        u32 c, nt;
+        msm::resolve(k.n ? k.n : 1, k.window, k.n_tables, &c, &nt);
+        ZK_CHECK_ARG(c >= 2 && c <= 24 && nt >= 1 && k.n * nt < (1ull << 31) && k.result_d != nullptr);
+        ZK_CHECK_ARG(k.n == 0 || (k.points_d != nullptr && k.scalars_d != nullptr));
+        b.task[t] = msm::make_task(k.n, c, nt);
+        b.task[t].points = k.points_d;
+        b.task[t].scalars = k.scalars_d;
+        b.task[t].result = k.result_d;
+    }
+    msm::finish_batch(b);
+    *out = b;
+    return cudaSuccess;
+}
+
+extern "C" unsigned long long zkp_msm_batch_workspace_size(const ZkpMsmTask *tasks, unsigned int ntasks) {
+    msm::Batch b;
+    if (build_batch(tasks, ntasks, &b) != cudaSuccess) return 0;
+    return msm::make_layout(b).total;
+}
+
+extern "C" cudaError_t zkp_msm_batch(const ZkpMsmTask *tasks, unsigned int ntasks, void *workspace_d,
+                                     unsigned long long workspace_bytes, cudaStream_t stream) {
+    msm::Batch b;
+    ZK_TRY(build_batch(tasks, ntasks, &b));
+    const msm::Layout l = msm::make_layout(b);
+    ZK_CHECK_ARG(workspace_d != nullptr && workspace_bytes >= l.total);
+    return msm::run_batch(b, l, reinterpret_cast<char *>(workspace_d), stream);
 }
 
 extern "C" cudaError_t zkp_msm_precompute_device(unsigned int *tables_d, unsigned long long n, unsigned int window,
@@ -545,6 +718,32 @@ extern "C" cudaError_t zkp_msm_precompute_device(unsigned int *tables_d, unsigne
         ZK_TRY(cudaGetLastError());
     }
     return cudaSuccess;
+}
+
+// device layout of one card's buffer for the reference ABI: points | scalars | result | batch ws
+struct CardLayout {
+    size_t points, scalars, result, ws, total;
+    msm::Batch batch;
+    msm::Layout l;
+};
+
+static CardLayout card_layout(u64 cnt, u32 c, u32 nt, char *base) {
+    CardLayout cl{};
+    size_t off = 0;
+    cl.points = off;
+    off += msm::align_up(cnt * nt * 64);
+    cl.scalars = off;
+    off += msm::align_up(cnt * 32);
+    cl.result = off;
+    off += 256;
+    cl.ws = off;
+    u32 *pts = base ? reinterpret_cast<u32 *>(base + cl.points) : nullptr;
+    u32 *sc = base ? reinterpret_cast<u32 *>(base + cl.scalars) : nullptr;
+    u32 *res = base ? reinterpret_cast<u32 *>(base + cl.result) : nullptr;
+    cl.batch = msm::single(pts, nt, sc, cnt, c, res);
+    cl.l = msm::make_layout(cl.batch);
+    cl.total = off + cl.l.total;
+    return cl;
 }
 
 extern "C" cudaError_t msm(void *const *buffers, unsigned long *buffer_sizes, unsigned long long len,
@@ -569,8 +768,7 @@ extern "C" cudaError_t msm(void *const *buffers, unsigned long *buffer_sizes, un
         for (u32 k = 0; k < num_cards; k++) {
             u64 lo, cnt;
             slice(k, &lo, &cnt);
-            msm::Config cfg = msm::make_config(cnt ? cnt : 1, c, nt);
-            buffer_sizes[k] = msm::make_layout(cfg, true, true).total;
+            buffer_sizes[k] = card_layout(cnt ? cnt : 1, c, nt, nullptr).total;
         }
         return cudaSuccess;
     }
@@ -585,18 +783,17 @@ extern "C" cudaError_t msm(void *const *buffers, unsigned long *buffer_sizes, un
         if (cnt == 0) continue;
         err = cudaSetDevice((int)cards[k]);
         if (err != cudaSuccess) break;
-        msm::Config cfg = msm::make_config(cnt, c, nt);
-        msm::Layout l = msm::make_layout(cfg, true, true);
-        char *ws = reinterpret_cast<char *>(buffers[k]);
-        u32 *d_points = reinterpret_cast<u32 *>(ws + l.points);
-        u32 *d_scalars = reinterpret_cast<u32 *>(ws + l.scalars);
-        u32 *d_result = reinterpret_cast<u32 *>(ws + l.result);
+        char *base = reinterpret_cast<char *>(buffers[k]);
+        CardLayout cl = card_layout(cnt, c, nt, base);
+        u32 *d_points = reinterpret_cast<u32 *>(base + cl.points);
+        u32 *d_scalars = reinterpret_cast<u32 *>(base + cl.scalars);
+        u32 *d_result = reinterpret_cast<u32 *>(base + cl.result);
         cudaStream_t st = cudaStreamPerThread;
         for (u32 j = 0; j < nt && err == cudaSuccess; j++)
             err = cudaMemcpyAsync(d_points + j * cnt * 16, h_points[j] + lo * 16, cnt * 64, cudaMemcpyHostToDevice, st);
         for (u32 b = 0; b < batches && err == cudaSuccess; b++) {
             err = cudaMemcpyAsync(d_scalars, h_scaler_batch[b] + lo * 8, cnt * 32, cudaMemcpyHostToDevice, st);
-            if (err == cudaSuccess) err = msm::run_device(cfg, l, ws, d_points, d_scalars, d_result, st);
+            if (err == cudaSuccess) err = msm::run_batch(cl.batch, cl.l, base + cl.ws, st);
             if (err == cudaSuccess)
                 err = cudaMemcpyAsync(partial[k].data() + b * 16, d_result, 64, cudaMemcpyDeviceToHost, st);
         }
@@ -608,10 +805,10 @@ extern "C" cudaError_t msm(void *const *buffers, unsigned long *buffer_sizes, un
         err = cudaSetDevice((int)cards[0]);
         u64 lo0, cnt0;
         slice(0, &lo0, &cnt0);
-        msm::Config cfg0 = msm::make_config(cnt0 ? cnt0 : 1, c, nt);
-        msm::Layout l0 = msm::make_layout(cfg0, true, true);
-        u32 *acc = reinterpret_cast<u32 *>(reinterpret_cast<char *>(buffers[0]) + l0.result);
-        u32 *other = acc + 16;  // the 256-byte aligned result slot has room for a second point
+        char *base0 = reinterpret_cast<char *>(buffers[0]);
+        CardLayout cl0 = card_layout(cnt0 ? cnt0 : 1, c, nt, base0);
+        u32 *acc = reinterpret_cast<u32 *>(base0 + cl0.result);
+        u32 *other = acc + 16;  // the 256-byte result slot holds a second point
         for (u32 b = 0; b < batches && err == cudaSuccess; b++) {
             err = cudaMemcpy(acc, partial[0].data() + b * 16, 64, cudaMemcpyHostToDevice);
             for (u32 k = 1; k < num_cards && err == cudaSuccess; k++) {

@@ -89,8 +89,7 @@ ZK_DI Fr omega_pow(const u32 *omegas, u64 e) {
     return r;
 }
 
-__global__ void __launch_bounds__(MAX_THREADS, 1) ntt_pass_kernel(PassArgs a) {
-    extern __shared__ u32 sm[];
+__device__ __forceinline__ void pass_body(const PassArgs &a, const u64 P, u32 *sm) {
     const u32 D = a.D;
     const u32 S = 1u << D;
     const u32 H = S >> 1;
@@ -99,7 +98,6 @@ __global__ void __launch_bounds__(MAX_THREADS, 1) ntt_pass_kernel(PassArgs a) {
     u32 *aux = tws + 8 * (H > 0 ? H : 1);  // 2 x 64 elements of shift tables (recompute twist)
     const u32 T = blockDim.x;
     const u32 tid = threadIdx.x;
-    const u64 P = (u64)blockIdx.y * gridDim.x + blockIdx.x;
     const u64 cmask = (1ull << a.lo) - 1;
     const u64 c = P & cmask;
     const u64 h = P >> a.lo;
@@ -133,17 +131,17 @@ __global__ void __launch_bounds__(MAX_THREADS, 1) ntt_pass_kernel(PassArgs a) {
     // ---- coset shift tables (pass 0): shift^(c + r*2^lo) = (shift^c * G^(r&63)) * G^(64*(r>>6))
     const bool preshift = (a.flags & F_PRESHIFT) != 0;
     if (preshift) {
-        if (tid < 128) {
+        for (u32 i = tid; i < 128; i += T) {
             Fr g = Fr::load_nc(a.shift);
             Fr G = g;
             for (u32 k = 0; k < a.lo; k++) G = Fr::mul(G, G);
             Fr w;
-            if (tid < 64) {
-                w = Fr::mul(Fr::pow_u64(g, c), Fr::pow_u64(G, tid));
+            if (i < 64) {
+                w = Fr::mul(Fr::pow_u64(g, c), Fr::pow_u64(G, i));
             } else {
-                w = Fr::pow_u64(G, (u64)(tid - 64) * 64);
+                w = Fr::pow_u64(G, (u64)(i - 64) * 64);
             }
-            sm_store(aux, 128, tid, w);
+            sm_store(aux, 128, i, w);
         }
         __syncthreads();
     }
@@ -191,10 +189,10 @@ __global__ void __launch_bounds__(MAX_THREADS, 1) ntt_pass_kernel(PassArgs a) {
     const bool twist = (a.flags & F_TWIST) != 0;
     if (twist && recompute) {
         // base = w_N^c with w_N = w^(2^(L-lo-D)); tables base^(k & 63), base^(64 * (k >> 6))
-        if (tid < 128) {
+        for (u32 i = tid; i < 128; i += T) {
             Fr base = omega_pow(a.omegas, c << (a.L - a.lo - D));
-            Fr w = tid < 64 ? Fr::pow_u64(base, tid) : Fr::pow_u64(base, (u64)(tid - 64) * 64);
-            sm_store(aux, 128, tid, w);
+            Fr w = i < 64 ? Fr::pow_u64(base, i) : Fr::pow_u64(base, (u64)(i - 64) * 64);
+            sm_store(aux, 128, i, w);
         }
         __syncthreads();
     }
@@ -226,6 +224,53 @@ __global__ void __launch_bounds__(MAX_THREADS, 1) ntt_pass_kernel(PassArgs a) {
         if (canon) x = x.canonical();
         const u64 gi = gbase + ((u64)q << a.lo);
         x.store(a.v.at(gi));
+    }
+}
+
+__global__ void __launch_bounds__(MAX_THREADS, 1) ntt_pass_kernel(PassArgs a) {
+    extern __shared__ u32 sm[];
+    pass_body(a, (u64)blockIdx.y * gridDim.x + blockIdx.x, sm);
+}
+
+// Batched form: one persistent launch runs the same pass of many transforms.  Work item w is
+// pencil w - first[t] of task t, where first[] is the exclusive prefix of the tasks' pencil
+// counts (first[ntasks] = total); each CTA walks items w = blockIdx.x, + gridDim.x, ...
+__global__ void __launch_bounds__(MAX_THREADS, 1) ntt_batch_pass_kernel(const PassArgs *args, const u64 *first,
+                                                                       u32 ntasks) {
+    extern __shared__ u32 sm[];
+    const u64 total = first[ntasks];
+    for (u64 w = blockIdx.x; w < total; w += gridDim.x) {
+        u32 lo = 0, hi = ntasks;  // largest t with first[t] <= w
+        while (hi - lo > 1) {
+            const u32 mid = (lo + hi) / 2;
+            if (first[mid] <= w) lo = mid; else hi = mid;
+        }
+        pass_body(args[lo], w - first[lo], sm);
+        __syncthreads();  // the next item reuses shared memory
+    }
+}
+
+// batched in-place bit reversal: element w of the concatenation belongs to task t
+__global__ void __launch_bounds__(256) bitrev_batch_kernel(const View *views, const u32 *logs, const u64 *first,
+                                                          u32 ntasks) {
+    const u64 total = first[ntasks];
+    const u64 stride = (u64)gridDim.x * blockDim.x;
+    for (u64 w = (u64)blockIdx.x * blockDim.x + threadIdx.x; w < total; w += stride) {
+        u32 lo = 0, hi = ntasks;
+        while (hi - lo > 1) {
+            const u32 mid = (lo + hi) / 2;
+            if (first[mid] <= w) lo = mid; else hi = mid;
+        }
+        const u64 i = w - first[lo];
+        const u32 L = logs[lo];
+        const u64 j = __brevll(i) >> (64 - L);
+        if (i < j) {
+            const View &v = views[lo];
+            u32 *pi = v.at(i), *pj = v.at(j);
+            Fr x = Fr::load(pi), y = Fr::load(pj);
+            y.store(pi);
+            x.store(pj);
+        }
     }
 }
 
@@ -294,6 +339,7 @@ inline Plan make_plan(u32 L) {
 }
 
 std::atomic<uint64_t> g_attr_done{0};
+std::atomic<uint64_t> g_batch_attr_done{0};
 
 inline size_t pass_smem(u32 D) {
     const size_t S = 1u << D, H = S > 1 ? S / 2 : 1;
@@ -327,6 +373,7 @@ cudaError_t launch_pass(const PassArgs &a, cudaStream_t stream) {
 cudaError_t run(const View &v, const View *src, u64 src_len, u32 L, const u32 *tw, const u32 *omegas,
                 const u32 *shift, const u32 *scale, cudaStream_t stream) {
     const Plan plan = make_plan(L);
+    profiler().begin(stream);
     for (u32 p = 0; p < plan.np; p++) {
         PassArgs a{};
         a.v = v;
@@ -351,6 +398,7 @@ cudaError_t run(const View &v, const View *src, u64 src_len, u32 L, const u32 *t
         if (omegas) f |= F_RECOMPUTE;
         a.flags = f;
         ZK_TRY(launch_pass(a, stream));
+        profiler().mark("ntt_pass", stream);
     }
     if (plan.np > 1) {
         const u64 n = 1ull << L;
@@ -358,6 +406,7 @@ cudaError_t run(const View &v, const View *src, u64 src_len, u32 L, const u32 *t
         const u32 grid = (u32)(blocks < (u64)num_sms() * 16 ? blocks : (u64)num_sms() * 16);
         bitrev_kernel<<<grid, 256, 0, stream>>>(v, L, n);
         ZK_TRY(cudaGetLastError());
+        profiler().mark("bitrev", stream);
     }
     return cudaSuccess;
 }
@@ -366,6 +415,8 @@ cudaError_t run(const View &v, const View *src, u64 src_len, u32 L, const u32 *t
 }  // namespace zk
 
 using namespace zk;
+
+ZK_DEFINE_PROFILER_API(zkp_ntt)
 
 extern "C" cudaError_t ssip_ntt(PolyPtr x, const unsigned int *twiddle, unsigned int log_len, cudaStream_t stream,
                                 const unsigned int, const unsigned int) {
@@ -398,6 +449,166 @@ extern "C" cudaError_t zkp_coset_lde(PolyPtr out, ConstPolyPtr in, const unsigne
     View vo, vi;
     ZK_CHECK_ARG(make_view(out, &vo) && make_view(in, &vi));
     return ntt::run(vo, &vi, in.len, log_out, twiddle, nullptr, shift_d, nullptr, stream);
+}
+
+// ------------------------------------------------------------------ batched form
+struct ZkpNttBatchPlan {
+    struct Phase {
+        ntt::PassArgs *args;
+        u64 *first;
+        u32 count;
+        size_t smem;
+        u32 threads;
+        u32 grid;
+    };
+    int device = 0;
+    std::vector<Phase> phases;
+    View *br_views = nullptr;
+    u32 *br_logs = nullptr;
+    u64 *br_first = nullptr;
+    u32 br_count = 0;
+    u64 br_total = 0;
+    void *mem = nullptr;
+};
+
+extern "C" cudaError_t zkp_ntt_batch_plan_create(const ZkpNttTask *tasks, unsigned int ntasks,
+                                                 ZkpNttBatchPlan **out) {
+    ZK_CHECK_ARG(out != nullptr && (ntasks == 0 || tasks != nullptr));
+    auto *plan = new ZkpNttBatchPlan();
+    cudaGetDevice(&plan->device);
+    // host images of every phase's tables, then one device allocation
+    std::vector<std::vector<ntt::PassArgs>> args;
+    std::vector<std::vector<u64>> firsts;
+    std::vector<View> br_views;
+    std::vector<u32> br_logs;
+    std::vector<u64> br_first{0};
+    for (u32 t = 0; t < ntasks; t++) {
+        const ZkpNttTask &task = tasks[t];
+        const u32 L = task.log_len;
+        View v;
+        if (L == 0 || L > 28 || task.x.len != (1ull << L) || task.twiddle == nullptr || !make_view(task.x, &v)) {
+            delete plan;
+            return cudaErrorInvalidValue;
+        }
+        const ntt::Plan p = ntt::make_plan(L);
+        for (u32 ph = 0; ph < p.np; ph++) {
+            if (args.size() <= ph) {
+                args.emplace_back();
+                firsts.emplace_back(1, 0);
+            }
+            ntt::PassArgs a{};
+            a.v = v;
+            a.tw = task.twiddle;
+            a.shift = task.shift_d;
+            a.scale = task.scale_d;
+            a.L = L;
+            a.D = p.D[ph];
+            a.lo = p.lo[ph];
+            u32 f = 0;
+            if (a.lo > 0) f |= ntt::F_TWIST;
+            if (p.np == 1) f |= ntt::F_NATURAL;
+            if (ph + 1 == p.np) {
+                f |= ntt::F_CANON;
+                if (task.scale_d) f |= ntt::F_POSTSCALE;
+            }
+            if (ph == 0 && task.shift_d) f |= ntt::F_PRESHIFT;
+            a.flags = f;
+            args[ph].push_back(a);
+            firsts[ph].push_back(firsts[ph].back() + (1ull << (L - a.D)));
+        }
+        if (p.np > 1) {
+            br_views.push_back(v);
+            br_logs.push_back(L);
+            br_first.push_back(br_first.back() + (1ull << L));
+        }
+    }
+    size_t bytes = 0;
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    for (size_t ph = 0; ph < args.size(); ph++)
+        bytes += al(args[ph].size() * sizeof(ntt::PassArgs)) + al(firsts[ph].size() * sizeof(u64));
+    bytes += al(br_views.size() * sizeof(View) + 16) + al(br_logs.size() * 4 + 16) + al(br_first.size() * 8);
+    cudaError_t err = cudaMalloc(&plan->mem, bytes ? bytes : 256);
+    if (err != cudaSuccess) {
+        delete plan;
+        return err;
+    }
+    char *base = reinterpret_cast<char *>(plan->mem);
+    size_t off = 0;
+    int max_smem = 0;
+    cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, plan->device);
+    err = ensure_smem_attr(ntt::ntt_batch_pass_kernel, (int)ntt::pass_smem(ntt::MAX_D), ntt::g_batch_attr_done);
+    for (size_t ph = 0; ph < args.size() && err == cudaSuccess; ph++) {
+        ZkpNttBatchPlan::Phase P{};
+        P.args = reinterpret_cast<ntt::PassArgs *>(base + off);
+        off += al(args[ph].size() * sizeof(ntt::PassArgs));
+        P.first = reinterpret_cast<u64 *>(base + off);
+        off += al(firsts[ph].size() * sizeof(u64));
+        P.count = (u32)args[ph].size();
+        u32 maxD = 1;
+        for (auto &a : args[ph]) maxD = a.D > maxD ? a.D : maxD;
+        P.smem = ntt::pass_smem(maxD);
+        const u32 H = (1u << maxD) >> 1;
+        P.threads = H < ntt::MAX_THREADS ? (H ? H : 1) : ntt::MAX_THREADS;
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ntt::ntt_batch_pass_kernel, (int)P.threads, P.smem);
+        if (per_sm < 1) per_sm = 1;
+        const u64 total = firsts[ph].back();
+        const u64 cap = (u64)num_sms() * per_sm;
+        P.grid = (u32)(total < cap ? total : cap);
+        err = cudaMemcpy(P.args, args[ph].data(), args[ph].size() * sizeof(ntt::PassArgs), cudaMemcpyHostToDevice);
+        if (err == cudaSuccess)
+            err = cudaMemcpy(P.first, firsts[ph].data(), firsts[ph].size() * sizeof(u64), cudaMemcpyHostToDevice);
+        plan->phases.push_back(P);
+    }
+    if (err == cudaSuccess && !br_views.empty()) {
+        plan->br_views = reinterpret_cast<View *>(base + off);
+        off += al(br_views.size() * sizeof(View) + 16);
+        plan->br_logs = reinterpret_cast<u32 *>(base + off);
+        off += al(br_logs.size() * 4 + 16);
+        plan->br_first = reinterpret_cast<u64 *>(base + off);
+        plan->br_count = (u32)br_views.size();
+        plan->br_total = br_first.back();
+        err = cudaMemcpy(plan->br_views, br_views.data(), br_views.size() * sizeof(View), cudaMemcpyHostToDevice);
+        if (err == cudaSuccess)
+            err = cudaMemcpy(plan->br_logs, br_logs.data(), br_logs.size() * 4, cudaMemcpyHostToDevice);
+        if (err == cudaSuccess)
+            err = cudaMemcpy(plan->br_first, br_first.data(), br_first.size() * 8, cudaMemcpyHostToDevice);
+    }
+    if (err != cudaSuccess) {
+        cudaFree(plan->mem);
+        delete plan;
+        return err;
+    }
+    *out = plan;
+    return cudaSuccess;
+}
+
+// launches only (no allocation, no host copies), so a stream capture can record it
+extern "C" cudaError_t zkp_ntt_batch_run(const ZkpNttBatchPlan *plan, cudaStream_t stream) {
+    ZK_CHECK_ARG(plan != nullptr);
+    for (const auto &P : plan->phases) {
+        if (P.count == 0 || P.grid == 0) continue;
+        ntt::ntt_batch_pass_kernel<<<P.grid, P.threads, P.smem, stream>>>(P.args, P.first, P.count);
+        ZK_TRY(cudaGetLastError());
+    }
+    if (plan->br_count) {
+        const u64 blocks = (plan->br_total / 2 + 255) / 256;
+        const u32 grid = (u32)(blocks < (u64)num_sms() * 16 ? blocks : (u64)num_sms() * 16);
+        ntt::bitrev_batch_kernel<<<grid, 256, 0, stream>>>(plan->br_views, plan->br_logs, plan->br_first,
+                                                          plan->br_count);
+        ZK_TRY(cudaGetLastError());
+    }
+    return cudaSuccess;
+}
+
+extern "C" void zkp_ntt_batch_plan_destroy(ZkpNttBatchPlan *plan) {
+    if (!plan) return;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(plan->device);
+    cudaFree(plan->mem);
+    cudaSetDevice(prev);
+    delete plan;
 }
 
 extern "C" unsigned int zkp_ntt_num_passes(unsigned int log_len) {

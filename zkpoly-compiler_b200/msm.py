@@ -145,3 +145,30 @@ class ResidentBases:
         check(_lib().zkp_msm_device(workspace.data_ptr(), workspace.numel(), self.tables.data_ptr(), self.n_tables,
                                     scalars.data_ptr(), self.n, self.window, result.data_ptr(),
                                     stream_handle(stream)), "zkp_msm_device")
+
+
+MAX_BATCH = 32
+
+
+class MsmBatch:
+    """Up to 32 MSMs of uneven sizes sharing every stage launch (zkp_msm_batch).
+
+    tasks: list of dicts with keys points (device (N, 16) int32, first table), scalars (device
+    (n, 8) int32), n, window (0 = auto), n_tables (default 1), result (device 16 int32).
+    The call allocates nothing once the workspace exists, so it can be graph-captured."""
+
+    def __init__(self, tasks):
+        from .native import ZkpMsmTask
+        assert 1 <= len(tasks) <= MAX_BATCH
+        self.tasks = tasks
+        self.arr = (ZkpMsmTask * len(tasks))()
+        for i, t in enumerate(tasks):
+            self.arr[i] = ZkpMsmTask(t["points"].data_ptr(), t.get("n_tables", 1), t["scalars"].data_ptr(), t["n"],
+                                     t.get("window", 0), t["result"].data_ptr())
+        self.ws_bytes = int(_lib().zkp_msm_batch_workspace_size(ctypes.cast(self.arr, ctypes.c_void_p), len(tasks)))
+        assert self.ws_bytes > 0, "invalid MSM batch"
+        self.workspace = torch.empty(self.ws_bytes, dtype=torch.uint8, device=tasks[0]["scalars"].device)
+
+    def run(self, stream=None):
+        check(_lib().zkp_msm_batch(ctypes.cast(self.arr, ctypes.c_void_p), len(self.tasks), self.workspace.data_ptr(),
+                                   self.ws_bytes, stream_handle(stream)), "zkp_msm_batch")

@@ -39,6 +39,12 @@ SIGNATURES = {
         "zkp_coset_lde": (cudaError_t, [PolyPtr, PolyPtr, c_void_p, ctypes.c_uint, ctypes.c_uint, c_void_p,
                                         c_void_p]),
         "zkp_ntt_num_passes": (ctypes.c_uint, [ctypes.c_uint]),
+        "zkp_ntt_batch_plan_create": (cudaError_t, [c_void_p, ctypes.c_uint, ctypes.POINTER(c_void_p)]),
+        "zkp_ntt_batch_run": (cudaError_t, [c_void_p, c_void_p]),
+        "zkp_ntt_batch_plan_destroy": (None, [c_void_p]),
+        "zkp_ntt_profile_enable": (None, [ctypes.c_int]),
+        "zkp_ntt_profile_read": (ctypes.c_int, [ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_char_p),
+                                                ctypes.c_int]),
     },
     "libmsm.so": {
         "msm": (cudaError_t, [ctypes.POINTER(c_void_p), ctypes.POINTER(ctypes.c_ulong), ctypes.c_ulonglong,
@@ -52,6 +58,17 @@ SIGNATURES = {
                                          ctypes.c_ulonglong, ctypes.c_uint, c_void_p, c_void_p]),
         "zkp_msm_precompute_device": (cudaError_t, [c_void_p, ctypes.c_ulonglong, ctypes.c_uint, ctypes.c_uint,
                                                     c_void_p]),
+        "zkp_msm_batch_workspace_size": (ctypes.c_ulonglong, [c_void_p, ctypes.c_uint]),
+        "zkp_msm_batch": (cudaError_t, [c_void_p, ctypes.c_uint, c_void_p, ctypes.c_ulonglong, c_void_p]),
+        "zkp_msm_profile_enable": (None, [ctypes.c_int]),
+        "zkp_msm_profile_read": (ctypes.c_int, [ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_char_p),
+                                                ctypes.c_int]),
+        "zkp_imad_probe": (cudaError_t, [ctypes.c_uint, ctypes.c_uint, c_void_p, c_void_p]),
+    },
+    "libzkp_gen.so": {
+        "zkp_gen_fr": (cudaError_t, [ctypes.c_ulonglong, ctypes.c_ulonglong, ctypes.c_ulonglong, c_void_p, c_void_p]),
+        "zkp_gen_points": (cudaError_t, [ctypes.c_ulonglong, ctypes.c_ulonglong, ctypes.c_ulonglong, c_void_p,
+                                         c_void_p, c_void_p]),
     },
     "libpoly.so": {
         "poly_add": (cudaError_t, [PolyPtr, PolyPtr, PolyPtr, c_void_p]),
@@ -69,6 +86,18 @@ SIGNATURES = {
         "scalar_pow": (cudaError_t, [c_void_p, ctypes.c_ulonglong, c_void_p]),
     },
 }
+
+
+class ZkpNttTask(ctypes.Structure):
+    """include/ntt.h ZkpNttTask"""
+    _fields_ = [("x", PolyPtr), ("twiddle", ctypes.c_void_p), ("log_len", ctypes.c_uint),
+                ("shift_d", ctypes.c_void_p), ("scale_d", ctypes.c_void_p)]
+
+
+class ZkpMsmTask(ctypes.Structure):
+    """include/msm.h ZkpMsmTask"""
+    _fields_ = [("points_d", ctypes.c_void_p), ("n_tables", ctypes.c_uint), ("scalars_d", ctypes.c_void_p),
+                ("n", ctypes.c_ulonglong), ("window", ctypes.c_uint), ("result_d", ctypes.c_void_p)]
 
 
 class CudaError(RuntimeError):
@@ -100,6 +129,20 @@ def load(name: str) -> ctypes.CDLL:
 def check(code: int, where: str) -> None:
     if code != 0:
         raise CudaError(code, where)
+
+
+def profile_enable(name: str, on: bool) -> None:
+    prefix = {"libntt.so": "zkp_ntt", "libmsm.so": "zkp_msm"}[name]
+    getattr(load(name), prefix + "_profile_enable")(int(on))
+
+
+def profile_read(name: str):
+    """[(stage, ms)] of the last call of the library while profiling was on."""
+    prefix = {"libntt.so": "zkp_ntt", "libmsm.so": "zkp_msm"}[name]
+    ms = (ctypes.c_float * 32)()
+    names = (ctypes.c_char_p * 32)()
+    k = getattr(load(name), prefix + "_profile_read")(ms, names, 32)
+    return [(names[i].decode(), ms[i]) for i in range(k)]
 
 
 def loaded_paths():

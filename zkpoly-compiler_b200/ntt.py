@@ -146,6 +146,40 @@ def coset_ntt(out: ScalarArray, coef: ScalarArray, shift: int = field.GENERATOR,
     coset_lde(out, coef, twiddle_table(_log2_exact(out.len), False), scalar_const(shift), stream)
 
 
+# ------------------------------------------------------------------ batched form
+class NttBatch:
+    """Many in-place transforms of uneven sizes as one graph-capturable launch sequence.
+
+    tasks: list of (ScalarArray, kind) with kind in {"ntt", "intt", "coset"}; a coset task
+    multiplies x[i] by GENERATOR^i before the forward transform (the input must already be
+    the zero-extended coefficient vector)."""
+
+    def __init__(self, tasks, shift: int = field.GENERATOR):
+        from .native import ZkpNttTask
+        lib = _lib()
+        arr = (ZkpNttTask * len(tasks))()
+        self._keep = []
+        for i, (x, kind) in enumerate(tasks):
+            log_n = _log2_exact(x.len)
+            inverse = kind == "intt"
+            tw = twiddle_table(log_n, inverse)
+            sh = scalar_const(shift) if kind == "coset" else None
+            sc = n_inv(log_n) if inverse else None
+            self._keep += [x, tw, sh, sc]
+            arr[i] = ZkpNttTask(x.poly_ptr(), tw.values.data_ptr(), log_n, _ptr(sh), _ptr(sc))
+        self._plan = ctypes.c_void_p()
+        check(lib.zkp_ntt_batch_plan_create(ctypes.cast(arr, ctypes.c_void_p), len(tasks),
+                                            ctypes.byref(self._plan)), "zkp_ntt_batch_plan_create")
+
+    def run(self, stream=None):
+        check(_lib().zkp_ntt_batch_run(self._plan, stream_handle(stream)), "zkp_ntt_batch_run")
+
+    def __del__(self):
+        if getattr(self, "_plan", None):
+            load(LIB).zkp_ntt_batch_plan_destroy(self._plan)
+            self._plan = None
+
+
 # ------------------------------------------------------------------ RegisteredFunction mirrors
 class SsipNtt:
     """core/src/ntt.rs:152-200"""
