@@ -100,18 +100,23 @@ def cpu_model():
 
 
 # ------------------------------------------------------------------ CPU (reference path)
-def cpu_reference(sample_msm_log=16, sample_ntt_log=20, reps=1):
+_CPU_INPUTS = {}
+
+
+def cpu_reference(sample_msm_log=22, sample_ntt_log=24, reps=1):
     """halo2 best_multiexp / best_fft restated (oracle), all host threads, bounded samples."""
     from oracle import oracle as orc
     orc.build()
     th = orc.threads()
-    s = orc.gen_fr(1, 1 << sample_msm_log)
-    p = orc.gen_points(2, 1 << sample_msm_log)
+    key = (sample_msm_log, sample_ntt_log)
+    if key not in _CPU_INPUTS:
+        _CPU_INPUTS[key] = (orc.gen_fr(1, 1 << sample_msm_log), orc.gen_points(2, 1 << sample_msm_log),
+                            orc.gen_fr(0, 1 << sample_ntt_log))
+    s, p, a = _CPU_INPUTS[key]
     t0 = time.perf_counter()
     for _ in range(reps):
         orc.best_multiexp(s, p)
     msm_t = (time.perf_counter() - t0) / reps
-    a = orc.gen_fr(0, 1 << sample_ntt_log)
     w = orc.root_of_unity(sample_ntt_log)
     t0 = time.perf_counter()
     for _ in range(reps):
@@ -176,7 +181,13 @@ def run_gpu(args):
         ntt_in = gen.fr(0, n_ntt, dev)
         x = zk.ScalarArray(ntt_in.clone())
         tw = zk.ntt.twiddle_table(NTT_LOG)
-        bases = zk.msm.ResidentBases(points, window=args.window)
+        if args.window:
+            win, nt = args.window, args.tables or 1
+        else:
+            win, nt = zk.tuner.msm_resident_config(n_msm)
+            if args.tables:
+                nt = args.tables
+        bases = zk.msm.ResidentBases(points, window=win, n_tables=nt)
         ws = bases.workspace()
         res = torch.zeros(16, dtype=torch.int32, device=dev)
     torch.cuda.synchronize()
@@ -248,12 +259,86 @@ def run_gpu(args):
     torch.cuda.synchronize()
     imad_per_s = 5 * sms * 8 * 256 * iters * 16 / (e0.elapsed_time(e1) / 1e3)
 
+    # ---- batched form (mixed NTT/MSM workload) and served form (Poisson arrivals)
+    batched = measure_batched(zk, args) if (not args.no_batched and rank == 0) else None
+    served = measure_served(zk, bases, args) if (not args.no_served and rank == 0) else None
+
     # ---- e2e through the reference C ABI from pinned host memory
+    e2e_msm_s = e2e_ntt_s = float("nan")
+    if not args.no_e2e:
+        e2e_msm_s, e2e_ntt_s = run_e2e(zk, native, lib_msm, scalars, points, ntt_in, tw, stream, dev, local, args,
+                                       n_msm, n_ntt)
+
+    # ---- CPU baseline (rank 0 at N=1)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_reference(args.ref_msm_log, args.ref_ntt_log)
+    emit(args, zk, rank, world, n_msm, n_ntt, ntt_ms, msm_ms, step_ms, pass_ms, bitrev_ms, stage_ms, imad_per_s,
+         e2e_msm_s, e2e_ntt_s, cpu, clocks, bases, batched, served)
+
+
+def measure_batched(zk, args, reps=3):
+    """64 NTTs (log2 n uniform on 10..20, forward / inverse / coset) + 16 MSMs (log2 n uniform
+    on 12..22), seed 3: per-call path vs one captured graph of the batched launches."""
+    import torch
+    w = zk.batched.MixedWorkload(seed=3)
+    w.build_batched()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    torch.cuda.synchronize()
+    w.run_plain()
+    torch.cuda.synchronize()
+    ev[0].record()
+    for _ in range(reps):
+        w.run_plain()
+    ev[1].record()
+    torch.cuda.synchronize()
+    w.run_batched()
+    torch.cuda.synchronize()
+    ev[2].record()
+    for _ in range(reps):
+        w.run_batched()
+    ev[3].record()
+    torch.cuda.synchronize()
+    plain_ms = ev[0].elapsed_time(ev[1]) / reps
+    bat_ms = ev[2].elapsed_time(ev[3]) / reps
+    work = w.work()
+    out = {"workload": "64 NTTs 2^10..2^20 (fwd/inv/coset) + 16 MSMs 2^12..2^22, seed 3",
+           "ntt_logs": w.ntt_logs, "msm_logs": w.msm_logs, "msm_windows": w.windows,
+           "plain_ms": plain_ms, "batched_ms": bat_ms, "speedup": plain_ms / bat_ms,
+           "tasks_per_s_plain": work["tasks"] / (plain_ms / 1e3), "tasks_per_s_batched": work["tasks"] / (bat_ms / 1e3),
+           "work": work}
+    del w
+    torch.cuda.empty_cache()
+    return out
+
+
+def measure_served(zk, bases, args):
+    """Poisson arrivals (50 req/s, k uniform on 14..22) of the prover-shaped program; the served
+    form (continuous batching, 8 slots, HBM admission) vs the plain path (one request at a time)."""
+    import torch
+    sched = zk.serving.poisson_schedule(args.served_requests, rate=50.0, k_lo=14, k_hi=22, seed=5)
+    out = {"workload": f"{args.served_requests} requests, Poisson 50 req/s, k uniform 14..22, program = "
+                       "3 INTT + coset NTT 4x + fused quotient + 4 MSM (one batch) + 2 evals",
+           "hbm_arena_gb": 48}
+    for name, inflight in (("served", 8), ("plain", 1)):
+        srv = zk.serving.Server(bases, hbm_bytes=48 << 30, max_inflight=inflight, ext_log=2, min_k=14, max_k=22)
+        # warm the constants / kernels once
+        srv.wait(srv.submit(14, 1))
+        _, summary = zk.serving.run_schedule(srv, sched)
+        srv.close()
+        out[name] = summary
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_e2e(zk, native, lib_msm, scalars, points, ntt_in, tw, stream, dev, local, args, n_msm, n_ntt):
+    import ctypes
+    import numpy as np
+    import torch
     h_scal = scalars.cpu().pin_memory()
     h_pts = points.cpu().pin_memory()
     h_ntt = ntt_in.cpu().pin_memory()
     h_out = torch.empty_like(h_ntt).pin_memory()
-    import ctypes
     cfg = zk.msm.MsmConfig(cards=[local])
     sizes = zk.msm.MSM(cfg).get_buffer_size(n_msm)
     buf = torch.empty(sizes[0], dtype=torch.uint8, device=dev)
@@ -287,14 +372,12 @@ def run_gpu(args):
             e2e_ntt()
         stream.synchronize()
         t2 = time.perf_counter()
-    e2e_msm_s = (t1 - t0) / args.steps
-    e2e_ntt_s = (t2 - t1) / args.steps
+    return (t1 - t0) / args.steps, (t2 - t1) / args.steps
 
-    # ---- CPU baseline (rank 0 at N=1)
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_reference(args.ref_msm_log, args.ref_ntt_log)
 
+def emit(args, zk, rank, world, n_msm, n_ntt, ntt_ms, msm_ms, step_ms, pass_ms, bitrev_ms, stage_ms, imad_per_s,
+         e2e_msm_s, e2e_ntt_s, cpu, clocks, bases, batched=None, served=None):
+    import torch
     if rank != 0:
         if world > 1:
             torch.distributed.destroy_process_group()
@@ -313,9 +396,11 @@ def run_gpu(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32 (BN254 Montgomery limbs, exact)",
         "data": "synthetic (seeded counter-based generator; points k_i*G)",
-        "config": {"workload": f"MSM n=2^{MSM_LOG} (BN254 G1, resident bases, window {bases.window}) + "
+        "config": {"workload": f"MSM n=2^{MSM_LOG} (BN254 G1, resident bases, window {bases.window}, "
+                               f"{bases.n_tables} precomputed tables) + "
                                f"NTT n=2^{NTT_LOG} (BN254 Fr, natural order)",
-                   "msm_n": n_msm, "ntt_n": n_ntt, "window": bases.window, "parallelism": f"replicas x{world}",
+                   "msm_n": n_msm, "ntt_n": n_ntt, "window": bases.window, "msm_tables": bases.n_tables,
+                   "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (NTT 512 MiB, MSM points 256 MiB + 537 MiB sorted digits)"},
         "msm": {"metric": f"MSM points/s (2^{MSM_LOG})", "value": world * n_msm / (msm_ms / 1e3),
                 "ms": msm_ms, "stages_ms": stage_ms},
@@ -336,13 +421,17 @@ def run_gpu(args):
             "ntt_pass": {"fr_mults_per_pass": (n_ntt // 2) * 12,
                          "frac": ((n_ntt // 2) * 12 / (pass_avg / 1e3)) / (imad_per_s / imad_per_mult)},
         },
-        "e2e": {"value": world * n_msm / e2e_msm_s, "unit": "points/s",
+        "e2e": {"value": world * n_msm / e2e_msm_s if e2e_msm_s == e2e_msm_s else None, "unit": "points/s",
                 "h2d_bytes_per_step": n_msm * (64 + 32) + n_ntt * 32, "d2h_bytes_per_step": 64 + n_ntt * 32,
-                "ntt_elems_per_s": world * n_ntt / e2e_ntt_s,
+                "ntt_elems_per_s": world * n_ntt / e2e_ntt_s if e2e_ntt_s == e2e_ntt_s else None,
                 "path": "msm(): reference C ABI, host tables in, host result out; ssip_ntt with H2D/D2H"},
         "gpu_launches": args.steps * (launches_per_ntt + launches_per_msm),
         "clocks": clocks.summary(),
     }
+    if batched:
+        line["batched"] = batched
+    if served:
+        line["served"] = served
     if cpu:
         line["cpu_baseline"] = {"value": cpu["msm_points_per_s"], "unit": "points/s", "cores": cpu["cores"],
                                 "kind": "port", "sample": cpu["msm_sample"] + "; " + cpu["ntt_sample"],
@@ -359,10 +448,19 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--window", type=int, default=0)
-    ap.add_argument("--ref-msm-log", type=int, default=16)
-    ap.add_argument("--ref-ntt-log", type=int, default=20)
+    ap.add_argument("--tables", type=int, default=0, help="precomputed point tables (0 = tuned / full)")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-served", action="store_true")
+    ap.add_argument("--served-requests", type=int, default=120)
+    ap.add_argument("--ref-msm-log", type=int, default=22)
+    ap.add_argument("--ref-ntt-log", type=int, default=24)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer C-ABI leg (profiling runs)")
+    ap.add_argument("--ntt-log", type=int, default=24)
+    ap.add_argument("--msm-log", type=int, default=22)
     args = ap.parse_args()
+    global MSM_LOG, NTT_LOG
+    MSM_LOG, NTT_LOG = args.msm_log, args.ntt_log
     if args.impl == "reference":
         run_reference_arm(args)
     else:

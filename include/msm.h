@@ -69,6 +69,8 @@ typedef struct ZkpMsmTask {
     unsigned long long n;
     unsigned int window;           /* 0 = choose */
     unsigned int *result_d;        /* 64-byte affine result */
+    unsigned long long table_stride; /* points between tables (0 = n): an MSM over the first n
+                                        points of longer resident tables */
 } ZkpMsmTask;
 
 unsigned long long zkp_msm_batch_workspace_size(const ZkpMsmTask *tasks, unsigned int ntasks);

@@ -56,6 +56,11 @@ cudaError_t zkp_ntt_ex(PolyPtr x, const unsigned int *twiddle, unsigned int log_
 cudaError_t zkp_coset_lde(PolyPtr out, ConstPolyPtr in, const unsigned int *twiddle, unsigned int log_in,
                           unsigned int log_out, const unsigned int *shift_d, cudaStream_t stream);
 
+/* Device twin of ssip_precompute: out_d[i] = unit^i for i < count, unit_d on the device;
+ * asynchronous on `stream`, no allocation. */
+cudaError_t zkp_ntt_roots_device(unsigned int *out_d, unsigned long long count, const unsigned int *unit_d,
+                                 cudaStream_t stream);
+
 /* Number of sub-transform passes + permutation passes the plan for 2^log_len uses. */
 unsigned int zkp_ntt_num_passes(unsigned int log_len);
 

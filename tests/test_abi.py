@@ -13,6 +13,7 @@ HEADER_LIB = {
     "msm.h": "libmsm.so",
     "poly.h": "libpoly.so",
     "zkp_gen.h": "libzkp_gen.so",
+    "zkp_runtime.h": "libzkp_runtime.so",
 }
 
 

@@ -143,6 +143,29 @@ inline Fe inv(const Params &P, const Fe &a) {
     return r;
 }
 
+// a^e for a 256-bit exponent (4 little-endian u64 limbs)
+inline Fe pow_big(const Params &P, const Fe &a, const uint64_t e[4]) {
+    Fe r = one(P);
+    for (int i = 255; i >= 0; i--) {
+        r = mul(P, r, r);
+        if ((e[i / 64] >> (i % 64)) & 1) r = mul(P, r, a);
+    }
+    return r;
+}
+
+// primitive 2^log_n-th root of unity of Fr, Montgomery form: (7^((r-1)/2^28))^(2^(28-log_n)),
+// inverted when `inverse` (compiler/src/utils.rs:51-77)
+inline Fe fr_root_of_unity(unsigned log_n, bool inverse) {
+    const Params &P = fr();
+    uint64_t t[4];
+    memcpy(t, P.p, 32);
+    t[0] -= 1;
+    for (int i = 0; i < 4; i++) t[i] = (t[i] >> 28) | (i < 3 ? (t[i + 1] << 36) : 0);
+    Fe root = pow_big(P, from_u64(P, 7), t);
+    for (unsigned i = log_n; i < 28; i++) root = mul(P, root, root);
+    return inverse ? inv(P, root) : root;
+}
+
 inline Fe load(const unsigned int *w) {
     Fe r;
     memcpy(r.l, w, 32);

@@ -48,6 +48,7 @@ struct Task {
     const u32 *scalars;  // n Montgomery scalars
     u32 *result;         // 64-byte affine result
     u64 n;
+    u64 stride;  // points between consecutive tables (>= n; tables may be longer than n)
     u32 n_tables;
     u32 c;    // window bits
     u32 W;    // logical windows = ceil(254 / c)
@@ -82,6 +83,7 @@ ZK_DI u32 find_task(const T *first, u32 ntasks, T x) {
 inline Task make_task(u64 n, u32 c, u32 n_tables) {
     Task t{};
     t.n = n;
+    t.stride = n;
     t.c = c;
     t.W = (SCALAR_BITS + c - 1) / c;
     t.n_tables = n_tables;
@@ -244,7 +246,7 @@ __global__ void __launch_bounds__(256) scatter_kernel(const Batch b, u32 *cursor
         for_each_digit(d, k, [&](u32 table, u32 key, bool neg) {
             const u32 pos = atomicAdd(cursor + kb + key, 1u);
             sorted_bucket[pos] = kb + key;
-            sorted_point[pos] = (u32)(table * k.n + i) | (neg ? 0x80000000u : 0u);
+            sorted_point[pos] = (u32)(table * k.stride + i) | (neg ? 0x80000000u : 0u);
         });
     }
 }
@@ -680,9 +682,11 @@ static cudaError_t build_batch(const ZkpMsmTask *tasks, unsigned int ntasks, msm
         const ZkpMsmTask &k = tasks[t];
         u32 c, nt;
         msm::resolve(k.n ? k.n : 1, k.window, k.n_tables, &c, &nt);
-        ZK_CHECK_ARG(c >= 2 && c <= 24 && nt >= 1 && k.n * nt < (1ull << 31) && k.result_d != nullptr);
+        const u64 stride = k.table_stride ? k.table_stride : k.n;
+        ZK_CHECK_ARG(c >= 2 && c <= 24 && nt >= 1 && stride >= k.n && stride * nt < (1ull << 31) && k.result_d != nullptr);
         ZK_CHECK_ARG(k.n == 0 || (k.points_d != nullptr && k.scalars_d != nullptr));
         b.task[t] = msm::make_task(k.n, c, nt);
+        b.task[t].stride = stride;
         b.task[t].points = k.points_d;
         b.task[t].scalars = k.scalars_d;
         b.task[t].result = k.result_d;

@@ -641,6 +641,15 @@ extern "C" cudaError_t distribute_powers(PolyPtr poly, const unsigned int *power
     return cudaGetLastError();
 }
 
+extern "C" cudaError_t zkp_ntt_roots_device(unsigned int *out_d, unsigned long long count, const unsigned int *unit_d,
+                                            cudaStream_t stream) {
+    if (count == 0) return cudaSuccess;
+    ZK_CHECK_ARG(out_d != nullptr && unit_d != nullptr);
+    const u64 threads = (count + 63) / 64;
+    ntt::powers_kernel<<<(u32)((threads + 255) / 256), 256, 0, stream>>>(out_d, unit_d, count);
+    return cudaGetLastError();
+}
+
 extern "C" cudaError_t ssip_precompute(unsigned int *twiddle, unsigned int len, const unsigned int *unit) {
     if (len == 0) return cudaSuccess;
     ZK_CHECK_ARG(twiddle != nullptr && unit != nullptr);

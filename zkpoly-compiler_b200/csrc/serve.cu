@@ -1,0 +1,518 @@
+// libzkp_runtime.so: continuous-batching request loop for prover-shaped programs (one GPU).
+//
+// Host-side structure (the reference's scheduler, scheduler/src/scheduler.rs:255-426, admits
+// whole programs by CPU-memory "versions" and runs one card per request; here admission is by
+// planned HBM footprint and requests share the GPU):
+//   - Arena: one device allocation carved by a first-fit free list with coalescing (the
+//     device-resident memory pool); a request's buffers are one contiguous block.
+//   - Scheduler thread: pops pending requests in arrival order while a slot (stream) is free
+//     and the request's footprint fits in the arena (with a short look-ahead so a small request
+//     can pass a large one that is waiting for memory), launches the program asynchronously on
+//     the slot's stream, records an event, and polls the events of running requests; on
+//     completion it copies the tiny results, frees the block and wakes waiters.
+//   - Device work of different requests overlaps because every request has its own stream;
+//     nothing inside a program synchronises the host.
+#include <cuda_runtime.h>
+#include <dlfcn.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/msm.h"
+#include "../../include/ntt.h"
+#include "../../include/poly.h"
+#include "../../include/zkp_gen.h"
+#include "../../include/zkp_runtime.h"
+#include "host_field.h"
+
+namespace {
+
+using u32 = uint32_t;
+using u64 = uint64_t;
+
+inline size_t al(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// ------------------------------------------------------------------ device arena
+class Arena {
+   public:
+    cudaError_t init(size_t bytes) {
+        size_ = al(bytes);
+        cudaError_t e = cudaMalloc(&base_, size_);
+        if (e != cudaSuccess) return e;
+        free_[0] = size_;
+        return cudaSuccess;
+    }
+    ~Arena() {
+        if (base_) cudaFree(base_);
+    }
+    // first fit; returns offset or SIZE_MAX
+    size_t alloc(size_t bytes) {
+        bytes = al(bytes);
+        for (auto it = free_.begin(); it != free_.end(); ++it) {
+            if (it->second >= bytes) {
+                size_t off = it->first, sz = it->second;
+                free_.erase(it);
+                if (sz > bytes) free_[off + bytes] = sz - bytes;
+                used_ += bytes;
+                peak_ = std::max(peak_, used_);
+                return off;
+            }
+        }
+        return SIZE_MAX;
+    }
+    void release(size_t off, size_t bytes) {
+        bytes = al(bytes);
+        used_ -= bytes;
+        auto it = free_.emplace(off, bytes).first;
+        auto next = std::next(it);
+        if (next != free_.end() && it->first + it->second == next->first) {
+            it->second += next->second;
+            free_.erase(next);
+        }
+        if (it != free_.begin()) {
+            auto prev = std::prev(it);
+            if (prev->first + prev->second == it->first) {
+                prev->second += it->second;
+                free_.erase(it);
+            }
+        }
+    }
+    char *ptr(size_t off) const { return reinterpret_cast<char *>(base_) + off; }
+    size_t size() const { return size_; }
+    size_t peak() const { return peak_; }
+
+   private:
+    void *base_ = nullptr;
+    size_t size_ = 0, used_ = 0, peak_ = 0;
+    std::map<size_t, size_t> free_;
+};
+
+// per-size constants resident for the server's lifetime
+struct SizeConsts {
+    u32 *inv_tw = nullptr;   // inverse roots, 2^(k-1) entries
+    u32 *fwd_tw = nullptr;   // forward roots of the extended size, 2^(k+ext-1) entries
+    u32 *ninv = nullptr;     // n^-1
+    u32 *zh_inv = nullptr;   // 2^ext values of 1/Z_H on the coset
+};
+
+// buffer plan of one request (offsets inside its arena block)
+struct Plan {
+    size_t a, b, c, z, e, q, x, args, results, msm_ws, eval_tmp0, eval_tmp1, total;
+    unsigned long msm_ws_bytes, eval_bytes;
+};
+
+struct Request {
+    long long ticket;
+    ZkpProverRequest req;
+    ZkpProverResult res;
+    size_t off = SIZE_MAX, bytes = 0;
+    int slot = -1;
+    bool done = false;
+};
+
+using FusedFn = cudaError_t (*)(const ConstPolyPtr *, const PolyPtr *, unsigned long long, bool, void *, cudaStream_t);
+
+}  // namespace
+
+struct ZkpServer {
+    ZkpServeConfig cfg{};
+    int device = 0;
+    const u32 *bases = nullptr;
+    u64 n_bases = 0;
+    Arena arena;
+    std::vector<SizeConsts> consts;  // index k
+    u32 *shift = nullptr;            // coset shift 7 (Montgomery)
+    void *fused_lib = nullptr;
+    FusedFn fused = nullptr;
+
+    struct Slot {
+        cudaStream_t stream = nullptr;
+        cudaEvent_t done = nullptr;
+        u32 *host = nullptr;    // pinned: results (4*16 + 2*8 words) + PolyPtr staging
+        Request *req = nullptr;
+    };
+    std::vector<Slot> slots;
+
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<Request *> pending;
+    std::unordered_map<long long, Request *> all;
+    long long next_ticket = 0;
+    bool stop = false;
+    std::thread worker;
+    std::chrono::steady_clock::time_point t0;
+    ZkpServeStats stats{};
+    u64 inflight = 0;
+
+    double now() const {
+        return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+};
+
+namespace {
+
+PolyPtr pp(u32 *p, u64 len) { return PolyPtr{p, len, 0, 0, len}; }
+ConstPolyPtr cp(const u32 *p, u64 len, u64 rotate = 0) { return ConstPolyPtr{p, len, rotate, 0, len}; }
+
+bool plan_request(ZkpServer *s, u32 k, Plan *p) {
+    const u64 n = 1ull << k, N = 1ull << (k + s->cfg.ext_log);
+    size_t off = 0;
+    auto take = [&](size_t b) {
+        size_t o = off;
+        off += al(b);
+        return o;
+    };
+    p->a = take(n * 32);
+    p->b = take(n * 32);
+    p->c = take(n * 32);
+    p->z = take(N * 32);
+    p->e = take(N * 32);
+    p->q = take(N * 32);
+    p->x = take(32);
+    p->args = take(8 * sizeof(PolyPtr));
+    p->results = take(4 * 64 + 2 * 32);
+    ZkpMsmTask t[4];
+    for (int i = 0; i < 4; i++)
+        t[i] = ZkpMsmTask{s->bases, s->cfg.msm_tables, s->bases /*sizes only*/, n, s->cfg.msm_window,
+                          reinterpret_cast<u32 *>(16), s->n_bases};
+    p->msm_ws_bytes = (unsigned long)zkp_msm_batch_workspace_size(t, 4);
+    if (p->msm_ws_bytes == 0) return false;
+    p->msm_ws = take(p->msm_ws_bytes);
+    unsigned long ev = 0;
+    if (poly_eval(nullptr, &ev, cp(nullptr, n), nullptr, nullptr, nullptr) != cudaSuccess) return false;
+    p->eval_bytes = ev;
+    p->eval_tmp0 = take(ev);
+    p->eval_tmp1 = take(ev);
+    p->total = off;
+    return true;
+}
+
+// the program of one request, launched asynchronously on `st`
+cudaError_t launch_program(ZkpServer *s, Request *r, ZkpServer::Slot &slot) {
+    const u32 k = r->req.k, ext = s->cfg.ext_log;
+    const u64 n = 1ull << k, N = 1ull << (k + ext);
+    Plan p;
+    plan_request(s, k, &p);
+    char *base = s->arena.ptr(r->off);
+    auto P = [&](size_t off) { return reinterpret_cast<u32 *>(base + off); };
+    cudaStream_t st = slot.stream;
+    const SizeConsts &sc = s->consts[k];
+    const u64 seed = r->req.seed * 8;
+#define RUN(x)                                   \
+    do {                                         \
+        cudaError_t e__ = (x);                   \
+        if (e__ != cudaSuccess) return e__;      \
+    } while (0)
+    if (r->req.inject_fault == 2) return cudaErrorLaunchFailure;  // host-side injected failure
+    // inputs (seeded, generated on the device)
+    RUN(zkp_gen_fr(seed + 0, 0, n, P(p.a), st));
+    RUN(zkp_gen_fr(seed + 1, 0, n, P(p.b), st));
+    RUN(zkp_gen_fr(seed + 2, 0, n, P(p.c), st));
+    RUN(zkp_gen_fr(seed + 3, 0, N, P(p.z), st));
+    RUN(zkp_gen_fr(seed + 4, 0, 1, P(p.x), st));
+    // three INTTs (n^-1 fused into the last pass)
+    RUN(zkp_ntt_ex(pp(P(p.a), n), sc.inv_tw, k, nullptr, sc.ninv, st));
+    RUN(zkp_ntt_ex(pp(P(p.b), n), sc.inv_tw, k, nullptr, sc.ninv, st));
+    RUN(zkp_ntt_ex(pp(P(p.c), n), sc.inv_tw, k, nullptr, sc.ninv, st));
+    // coset NTT of c on the extended domain
+    RUN(zkp_coset_lde(pp(P(p.e), N), cp(P(p.c), n), sc.fwd_tw, k, k + ext, s->shift, st));
+    // fused quotient: vars = [e, e, e, z, z(wX), zh_inv], mut = [q]
+    PolyPtr *stage = reinterpret_cast<PolyPtr *>(slot.host + 96);
+    stage[0] = pp(P(p.e), N);
+    stage[1] = pp(P(p.e), N);
+    stage[2] = pp(P(p.e), N);
+    stage[3] = pp(P(p.z), N);
+    stage[4] = PolyPtr{P(p.z), N, N - (1ull << ext), 0, N};  // element i = z[(i + 2^ext) mod N]
+    stage[5] = PolyPtr{sc.zh_inv, 1ull << ext, 0, 0, 1ull << ext};
+    stage[6] = pp(P(p.q), N);
+    RUN(cudaMemcpyAsync(P(p.args), stage, 7 * sizeof(PolyPtr), cudaMemcpyHostToDevice, st));
+    const PolyPtr *dargs = reinterpret_cast<const PolyPtr *>(P(p.args));
+    RUN(s->fused(reinterpret_cast<const ConstPolyPtr *>(dargs), dargs + 6, N, true, nullptr, st));
+    // four MSMs over the resident bases in one batched launch set
+    const u32 nt = s->cfg.msm_tables, w = s->cfg.msm_window;
+    ZkpMsmTask t[4] = {
+        {s->bases, nt, P(p.a), n, w, P(p.results) + 0, s->n_bases},
+        {s->bases, nt, P(p.b), n, w, P(p.results) + 16, s->n_bases},
+        {s->bases, nt, P(p.c), n, w, P(p.results) + 32, s->n_bases},
+        {s->bases, nt, P(p.q), n, w, P(p.results) + 48, s->n_bases},
+    };
+    RUN(zkp_msm_batch(t, 4, P(p.msm_ws), p.msm_ws_bytes, st));
+    // two evaluations
+    unsigned long eb = p.eval_bytes;
+    RUN(poly_eval(P(p.eval_tmp0), &eb, cp(P(p.a), n), P(p.results) + 64, P(p.x), st));
+    RUN(poly_eval(P(p.eval_tmp1), &eb, cp(P(p.b), n), P(p.results) + 72, P(p.x), st));
+    RUN(cudaMemcpyAsync(slot.host, P(p.results), 4 * 64 + 2 * 32, cudaMemcpyDeviceToHost, st));
+    RUN(cudaEventRecord(slot.done, st));
+#undef RUN
+    return cudaSuccess;
+}
+
+void finish(ZkpServer *s, Request *r, int status) {
+    r->res.status = status;
+    r->res.done_s = s->now();
+    r->done = true;
+    if (status == 0)
+        s->stats.completed++;
+    else
+        s->stats.failed++;
+}
+
+void worker_loop(ZkpServer *s) {
+    cudaSetDevice(s->device);
+    std::unique_lock<std::mutex> lk(s->mu);
+    while (true) {
+        bool progressed = false;
+        // completions
+        for (auto &slot : s->slots) {
+            if (!slot.req) continue;
+            cudaError_t q = cudaEventQuery(slot.done);
+            if (q == cudaErrorNotReady) continue;
+            Request *r = slot.req;
+            if (q == cudaSuccess) {
+                memcpy(r->res.msm, slot.host, sizeof(r->res.msm));
+                memcpy(r->res.evals, slot.host + 64, sizeof(r->res.evals));
+                finish(s, r, 0);
+            } else {
+                finish(s, r, -3);
+            }
+            s->arena.release(r->off, r->bytes);
+            slot.req = nullptr;
+            s->inflight--;
+            progressed = true;
+        }
+        if (progressed) s->cv_done.notify_all();
+        // admission: arrival order, look-ahead of 8 for a request that fits
+        for (size_t idx = 0; idx < s->pending.size() && idx < 8;) {
+            int free_slot = -1;
+            for (size_t i = 0; i < s->slots.size(); i++)
+                if (!s->slots[i].req) {
+                    free_slot = (int)i;
+                    break;
+                }
+            if (free_slot < 0) break;
+            Request *r = s->pending[idx];
+            if (r->req.inject_fault == 1) {  // host-side injected allocation refusal
+                s->pending.erase(s->pending.begin() + idx);
+                r->res.start_s = s->now();
+                finish(s, r, -4);
+                s->cv_done.notify_all();
+                continue;
+            }
+            size_t off = s->arena.alloc(r->bytes);
+            if (off == SIZE_MAX) {
+                idx++;
+                continue;
+            }
+            s->pending.erase(s->pending.begin() + idx);
+            r->off = off;
+            r->slot = free_slot;
+            r->res.start_s = s->now();
+            auto &slot = s->slots[free_slot];
+            slot.req = r;
+            s->inflight++;
+            s->stats.peak_inflight = std::max<u64>(s->stats.peak_inflight, s->inflight);
+            s->stats.peak_bytes = s->arena.peak();
+            cudaError_t e = launch_program(s, r, slot);
+            if (e != cudaSuccess) {
+                // the request fails alone: drain what was queued on its stream, release it
+                cudaStreamSynchronize(slot.stream);
+                cudaGetLastError();
+                s->arena.release(r->off, r->bytes);
+                slot.req = nullptr;
+                s->inflight--;
+                finish(s, r, -3);
+                s->cv_done.notify_all();
+            }
+        }
+        if (s->stop && s->pending.empty() && s->inflight == 0) break;
+        if (s->inflight > 0)
+            s->cv_work.wait_for(lk, std::chrono::microseconds(50));
+        else
+            s->cv_work.wait_for(lk, std::chrono::milliseconds(5));
+    }
+}
+
+}  // namespace
+
+extern "C" unsigned long long zkp_serve_footprint(const ZkpServer *s, unsigned int k) {
+    Plan p;
+    if (!plan_request(const_cast<ZkpServer *>(s), k, &p)) return 0;
+    return p.total;
+}
+
+extern "C" cudaError_t zkp_serve_create(const ZkpServeConfig *cfg, const unsigned int *bases_d,
+                                        unsigned long long n_bases, ZkpServer **out) {
+    if (!cfg || !out || !bases_d || cfg->max_inflight == 0 || cfg->msm_tables == 0 ||
+        (cfg->msm_tables > 1 && cfg->msm_window == 0) || cfg->min_k < 1 || cfg->max_k > 26 ||
+        cfg->min_k > cfg->max_k || cfg->ext_log < 1 || cfg->ext_log > 3 || n_bases < (1ull << cfg->max_k))
+        return cudaErrorInvalidValue;
+    auto *s = new ZkpServer();
+    s->cfg = *cfg;
+    s->t0 = std::chrono::steady_clock::now();
+    cudaGetDevice(&s->device);
+    s->bases = bases_d;
+    s->n_bases = n_bases;
+    // fused quotient kernel, generated next to this library (lib/fused/)
+    Dl_info info;
+    std::string dir = ".";
+    if (dladdr(reinterpret_cast<void *>(&zkp_serve_create), &info) && info.dli_fname) {
+        dir = info.dli_fname;
+        dir = dir.substr(0, dir.find_last_of('/'));
+    }
+    s->fused_lib = dlopen((dir + "/fused/libzkp_quotient_z8.so").c_str(), RTLD_NOW | RTLD_LOCAL);
+    if (s->fused_lib) s->fused = reinterpret_cast<FusedFn>(dlsym(s->fused_lib, "zkp_quotient_z8"));
+    if (!s->fused) {
+        delete s;
+        return cudaErrorSharedObjectSymbolNotFound;
+    }
+    cudaError_t e = s->arena.init(cfg->hbm_bytes);
+    // per-size constants
+    const zkh::Params &F = zkh::fr();
+    s->consts.resize(cfg->max_k + 1);
+    u32 *tmp = nullptr;
+    if (e == cudaSuccess) e = cudaMalloc(&tmp, 32);
+    if (e == cudaSuccess) e = cudaMalloc(&s->shift, 32);
+    if (e == cudaSuccess) {
+        zkh::Fe g = zkh::from_u64(F, 7);
+        e = cudaMemcpy(s->shift, g.l, 32, cudaMemcpyHostToDevice);
+    }
+    const u32 ext = cfg->ext_log;
+    for (u32 k = cfg->min_k; k <= cfg->max_k && e == cudaSuccess; k++) {
+        SizeConsts &c = s->consts[k];
+        const u64 n = 1ull << k;
+        e = cudaMalloc(&c.inv_tw, (n / 2) * 32);
+        if (e == cudaSuccess) e = cudaMalloc(&c.fwd_tw, (n << ext) / 2 * 32);
+        if (e == cudaSuccess) e = cudaMalloc(&c.ninv, 32);
+        if (e == cudaSuccess) e = cudaMalloc(&c.zh_inv, (32u << ext));
+        if (e != cudaSuccess) break;
+        zkh::Fe wi = zkh::fr_root_of_unity(k, true);
+        e = cudaMemcpy(tmp, wi.l, 32, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = zkp_ntt_roots_device(c.inv_tw, n / 2, tmp, 0);
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+        zkh::Fe wf = zkh::fr_root_of_unity(k + ext, false);
+        if (e == cudaSuccess) e = cudaMemcpy(tmp, wf.l, 32, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = zkp_ntt_roots_device(c.fwd_tw, (n << ext) / 2, tmp, 0);
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+        zkh::Fe ninv = zkh::inv(F, zkh::from_u64(F, n));
+        if (e == cudaSuccess) e = cudaMemcpy(c.ninv, ninv.l, 32, cudaMemcpyHostToDevice);
+        // 1/Z_H at g w_(k+ext)^j, Z_H(X) = X^n - 1: (g^n w^(j n) - 1)^-1 for j < 2^ext
+        std::vector<zkh::Fe> zh(1u << ext);
+        zkh::Fe gn = zkh::pow(F, zkh::from_u64(F, 7), n);
+        zkh::Fe wn = zkh::pow(F, wf, n);
+        zkh::Fe acc = gn;
+        for (u32 j = 0; j < (1u << ext); j++) {
+            zkh::Fe d = acc;
+            // d - 1 (canonical subtraction of the Montgomery one)
+            zkh::Fe one = zkh::one(F);
+            uint64_t t[4];
+            if (zkh::sub4(t, d.l, one.l)) zkh::add4(t, t, F.p);
+            memcpy(d.l, t, 32);
+            zh[j] = zkh::inv(F, d);
+            acc = zkh::mul(F, acc, wn);
+        }
+        if (e == cudaSuccess) e = cudaMemcpy(c.zh_inv, zh.data(), (32u << ext), cudaMemcpyHostToDevice);
+    }
+    if (tmp) cudaFree(tmp);
+    s->slots.resize(cfg->max_inflight);
+    for (auto &slot : s->slots) {
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&slot.stream, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&slot.done, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaMallocHost(&slot.host, 4096);
+    }
+    if (e != cudaSuccess) {
+        zkp_serve_destroy(s);
+        return e;
+    }
+    s->stats.arena_bytes = s->arena.size();
+    s->worker = std::thread(worker_loop, s);
+    *out = s;
+    return cudaSuccess;
+}
+
+extern "C" long long zkp_serve_submit(ZkpServer *s, const ZkpProverRequest *req) {
+    if (!s || !req) return -1;
+    auto *r = new Request();
+    r->req = *req;
+    memset(&r->res, 0, sizeof(r->res));
+    std::lock_guard<std::mutex> g(s->mu);
+    if (s->stop) {
+        delete r;
+        return -1;
+    }
+    r->ticket = s->next_ticket++;
+    r->res.submit_s = s->now();
+    s->all[r->ticket] = r;
+    Plan p;
+    if (req->k < s->cfg.min_k || req->k > s->cfg.max_k || !plan_request(s, req->k, &p)) {
+        finish(s, r, -1);
+        s->cv_done.notify_all();
+        return r->ticket;
+    }
+    r->bytes = p.total;
+    r->res.footprint = p.total;
+    if (al(p.total) > s->arena.size()) {
+        finish(s, r, -2);
+        s->cv_done.notify_all();
+        return r->ticket;
+    }
+    s->pending.push_back(r);
+    s->cv_work.notify_one();
+    return r->ticket;
+}
+
+extern "C" int zkp_serve_wait(ZkpServer *s, long long ticket, ZkpProverResult *out, double timeout_s) {
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->all.find(ticket);
+    if (it == s->all.end()) return -1;
+    Request *r = it->second;
+    auto deadline = std::chrono::steady_clock::now() + std::chrono::duration<double>(timeout_s);
+    while (!r->done) {
+        if (s->cv_done.wait_until(lk, deadline) == std::cv_status::timeout && !r->done) return 1;
+    }
+    if (out) *out = r->res;
+    return 0;
+}
+
+extern "C" void zkp_serve_stats(const ZkpServer *s, ZkpServeStats *out) {
+    auto *m = const_cast<ZkpServer *>(s);
+    std::lock_guard<std::mutex> g(m->mu);
+    *out = s->stats;
+    out->peak_bytes = s->arena.peak();
+}
+
+extern "C" double zkp_serve_now(const ZkpServer *s) { return s->now(); }
+
+extern "C" void zkp_serve_destroy(ZkpServer *s) {
+    if (!s) return;
+    {
+        std::lock_guard<std::mutex> g(s->mu);
+        s->stop = true;
+    }
+    s->cv_work.notify_all();
+    if (s->worker.joinable()) s->worker.join();
+    for (auto &slot : s->slots) {
+        if (slot.stream) cudaStreamDestroy(slot.stream);
+        if (slot.done) cudaEventDestroy(slot.done);
+        if (slot.host) cudaFreeHost(slot.host);
+    }
+    for (auto &c : s->consts) {
+        cudaFree(c.inv_tw);
+        cudaFree(c.fwd_tw);
+        cudaFree(c.ninv);
+        cudaFree(c.zh_inv);
+    }
+    if (s->shift) cudaFree(s->shift);
+    for (auto &kv : s->all) delete kv.second;
+    if (s->fused_lib) dlclose(s->fused_lib);
+    delete s;
+}

@@ -164,7 +164,7 @@ class MsmBatch:
         self.arr = (ZkpMsmTask * len(tasks))()
         for i, t in enumerate(tasks):
             self.arr[i] = ZkpMsmTask(t["points"].data_ptr(), t.get("n_tables", 1), t["scalars"].data_ptr(), t["n"],
-                                     t.get("window", 0), t["result"].data_ptr())
+                                     t.get("window", 0), t["result"].data_ptr(), t.get("table_stride", 0))
         self.ws_bytes = int(_lib().zkp_msm_batch_workspace_size(ctypes.cast(self.arr, ctypes.c_void_p), len(tasks)))
         assert self.ws_bytes > 0, "invalid MSM batch"
         self.workspace = torch.empty(self.ws_bytes, dtype=torch.uint8, device=tasks[0]["scalars"].device)

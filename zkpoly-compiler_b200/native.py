@@ -70,6 +70,15 @@ SIGNATURES = {
         "zkp_gen_points": (cudaError_t, [ctypes.c_ulonglong, ctypes.c_ulonglong, ctypes.c_ulonglong, c_void_p,
                                          c_void_p, c_void_p]),
     },
+    "libzkp_runtime.so": {
+        "zkp_serve_create": (cudaError_t, [c_void_p, c_void_p, ctypes.c_ulonglong, ctypes.POINTER(c_void_p)]),
+        "zkp_serve_submit": (ctypes.c_longlong, [c_void_p, c_void_p]),
+        "zkp_serve_footprint": (ctypes.c_ulonglong, [c_void_p, ctypes.c_uint]),
+        "zkp_serve_wait": (ctypes.c_int, [c_void_p, ctypes.c_longlong, c_void_p, ctypes.c_double]),
+        "zkp_serve_stats": (None, [c_void_p, c_void_p]),
+        "zkp_serve_now": (ctypes.c_double, [c_void_p]),
+        "zkp_serve_destroy": (None, [c_void_p]),
+    },
     "libpoly.so": {
         "poly_add": (cudaError_t, [PolyPtr, PolyPtr, PolyPtr, c_void_p]),
         "poly_sub": (cudaError_t, [PolyPtr, PolyPtr, PolyPtr, c_void_p]),
@@ -97,7 +106,30 @@ class ZkpNttTask(ctypes.Structure):
 class ZkpMsmTask(ctypes.Structure):
     """include/msm.h ZkpMsmTask"""
     _fields_ = [("points_d", ctypes.c_void_p), ("n_tables", ctypes.c_uint), ("scalars_d", ctypes.c_void_p),
-                ("n", ctypes.c_ulonglong), ("window", ctypes.c_uint), ("result_d", ctypes.c_void_p)]
+                ("n", ctypes.c_ulonglong), ("window", ctypes.c_uint), ("result_d", ctypes.c_void_p),
+                ("table_stride", ctypes.c_ulonglong)]
+
+
+class ZkpServeConfig(ctypes.Structure):
+    _fields_ = [("hbm_bytes", ctypes.c_ulonglong), ("max_inflight", ctypes.c_uint), ("ext_log", ctypes.c_uint),
+                ("min_k", ctypes.c_uint), ("max_k", ctypes.c_uint), ("msm_window", ctypes.c_uint),
+                ("msm_tables", ctypes.c_uint)]
+
+
+class ZkpProverRequest(ctypes.Structure):
+    _fields_ = [("k", ctypes.c_uint), ("seed", ctypes.c_ulonglong), ("inject_fault", ctypes.c_uint)]
+
+
+class ZkpProverResult(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("msm", (ctypes.c_uint * 16) * 4), ("evals", (ctypes.c_uint * 8) * 2),
+                ("submit_s", ctypes.c_double), ("start_s", ctypes.c_double), ("done_s", ctypes.c_double),
+                ("footprint", ctypes.c_ulonglong)]
+
+
+class ZkpServeStats(ctypes.Structure):
+    _fields_ = [("completed", ctypes.c_ulonglong), ("failed", ctypes.c_ulonglong),
+                ("peak_inflight", ctypes.c_ulonglong), ("peak_bytes", ctypes.c_ulonglong),
+                ("arena_bytes", ctypes.c_ulonglong)]
 
 
 class CudaError(RuntimeError):

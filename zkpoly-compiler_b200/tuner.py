@@ -49,10 +49,21 @@ def _save():
 
 
 def msm_window(n: int) -> int:
-    """Tuned window for n points if known, else 0 (the library's cost model)."""
+    """Tuned window for n points (one table) if known, else 0 (the library's cost model)."""
     log_n = max(1, (n - 1).bit_length())
     entry = _load().get(_device_key(), {}).get("msm_window", {}).get(str(log_n))
     return int(entry) if entry else 0
+
+
+def msm_resident_config(n: int):
+    """(window, n_tables) for resident bases of n points: the tuned pair if known, else full
+    precomputation (one table per window, so no doubling chain between windows) at c = 16."""
+    log_n = max(1, (n - 1).bit_length())
+    entry = _load().get(_device_key(), {}).get("msm_resident", {}).get(str(log_n))
+    if entry:
+        return int(entry[0]), int(entry[1])
+    c = 16
+    return c, (254 + c - 1) // c
 
 
 def _time(fn, reps=3) -> float:
@@ -93,3 +104,27 @@ def tune_msm(log_ns=range(12, 23), candidates=range(8, 21), bases=None) -> dict:
         _load().setdefault(_device_key(), {})["msm_window"] = out
         _save()
     return out
+
+
+def tune_msm_resident(log_n: int = 22, windows=(13, 14, 15, 16, 17, 18, 19, 20), full_only: bool = True,
+                      bases=None) -> tuple:
+    """Times zkp_msm_device over precomputed tables (one per window when full_only) for each
+    window width and caches the fastest (window, n_tables) for resident bases of 2^log_n."""
+    from . import gen, msm
+    n = 1 << log_n
+    pts = bases if bases is not None else gen.points(2, n)
+    s = gen.fr(78, n)
+    res = torch.zeros(16, dtype=torch.int32, device="cuda")
+    results = {}
+    for c in windows:
+        nt = (254 + c - 1) // c if full_only else 1
+        rb = msm.ResidentBases(pts, window=c, n_tables=nt)
+        ws = rb.workspace()
+        results[(c, nt)] = _time(lambda: rb.msm(s, res, ws), reps=2)
+        del rb, ws
+        torch.cuda.empty_cache()
+    best = min(results, key=results.get)
+    with _lock:
+        _load().setdefault(_device_key(), {}).setdefault("msm_resident", {})[str(log_n)] = list(best)
+        _save()
+    return best, {f"{c}x{nt}": t for (c, nt), t in results.items()}
