@@ -61,6 +61,12 @@ cudaError_t zkp_coset_lde(PolyPtr out, ConstPolyPtr in, const unsigned int *twid
 cudaError_t zkp_ntt_roots_device(unsigned int *out_d, unsigned long long count, const unsigned int *unit_d,
                                  cudaStream_t stream);
 
+/* Plan tuning (no counterpart in the reference): caps the digit width of the passes used for
+ * transforms of 2^log_len elements (log_len 0: every size) at max_digit in [4, 12] (0 restores
+ * the default 12).  Each pass transforms 2^D-element pencils in shared memory, D <= max_digit;
+ * a smaller cap means more passes of smaller CTAs.  Plans made after the call use it. */
+cudaError_t zkp_ntt_set_max_digit(unsigned int log_len, unsigned int max_digit);
+
 /* Number of sub-transform passes + permutation passes the plan for 2^log_len uses. */
 unsigned int zkp_ntt_num_passes(unsigned int log_len);
 

@@ -21,6 +21,9 @@ cudaError_t poly_add(PolyPtr r, ConstPolyPtr a, ConstPolyPtr b, cudaStream_t str
 cudaError_t poly_sub(PolyPtr r, ConstPolyPtr a, ConstPolyPtr b, cudaStream_t stream);
 cudaError_t poly_mul(PolyPtr r, ConstPolyPtr a, ConstPolyPtr b, cudaStream_t stream);
 
+/* r[i] = a[i]^2 (addition, no counterpart in the reference; the dedicated Montgomery squaring) */
+cudaError_t zkp_poly_square(PolyPtr r, ConstPolyPtr a, cudaStream_t stream);
+
 /* all ones (Lagrange one), [1, 0, ...] (coefficient one), all zeros (poly.h:10-14) */
 cudaError_t poly_one_lagrange(PolyPtr target, cudaStream_t stream);
 cudaError_t poly_one_coef(PolyPtr target, cudaStream_t stream);

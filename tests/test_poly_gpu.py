@@ -126,3 +126,17 @@ def test_scalar_inv_and_pow(zk, orc):
     z = scal(zk, np.zeros(4, dtype=np.uint64))
     zk.poly.inv_scalar(z)
     assert not z.cpu().numpy().any()
+
+
+def test_square_matches_mul(zk, orc):
+    """The dedicated Montgomery squaring equals a * a bit for bit (edge values included)."""
+    n = 20000
+    a = orc.gen_fr(13, n)
+    M_limbs = orc.int_to_limbs(M - 1)
+    a[0] = 0
+    a[1] = M_limbs                      # m - 1
+    a[2] = orc.int_to_limbs(1)
+    a[3] = orc.int_to_limbs((1 << 253) + 12345)
+    r = zk.ScalarArray.zeros(n)
+    zk.poly.poly_square(r, dev(zk, a))
+    assert np.array_equal(r.numpy_u64(), orc.vec_mul(a, a))

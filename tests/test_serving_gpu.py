@@ -129,3 +129,20 @@ def test_poisson_load_smoke(zk, bases):
     finally:
         srv.close()
     assert summary["ok"] == 24 and summary["p99_ms"] >= summary["p50_ms"] > 0
+
+
+def test_per_call_path_matches_served(zk, bases):
+    """The plain per-call path (reference-ABI MSM with host arrays) gives the served results."""
+    prover = zk.serving.PerCallProver(bases, ext_log=2)
+    srv = server(zk, bases, 4)
+    try:
+        reqs = [(10, 41), (13, 42), (14, 43)]
+        tickets = [(k, seed, srv.submit(k, seed)) for k, seed in reqs]
+        for k, seed, t in tickets:
+            r = srv.wait(t)
+            assert r.status == 0
+            assert np.array_equal(prover.run(k, seed), zk.serving.result_words(r)), (k, seed)
+    finally:
+        srv.close()
+    words, summary = zk.serving.run_schedule_per_call(prover, [(0.0, 10, 41), (0.01, 11, 44)])
+    assert summary["ok"] == 2 and summary["p99_ms"] >= summary["p50_ms"] > 0

@@ -4,11 +4,14 @@ The mixed workload (seeded): `n_ntt` transforms with log2 sizes uniform on [ntt_
 kinds uniform over forward / inverse / coset, and `n_msm` MSMs with log2 sizes uniform on
 [msm_lo, msm_hi] over prefixes of one resident base array.
 
-plain:   the per-call path - one ssip_ntt / zkp_ntt_ex / zkp_msm_device call per task, in order,
-         on one stream (what a caller of the reference ABI does).
+plain (reference ABI): the per-call path as the reference's runtime drives it - one
+         ssip_ntt / zkp_ntt_ex call per transform on the device buffer, and one `msm` call per
+         MSM with host scalars and a host point table (core/src/msm.rs:302-369), in order.
+plain (device): the same per-call order, but each MSM is zkp_msm_device over device-resident
+         bases (one table) - the per-call path with the host copies taken out.
 batched: one NttBatch plan (a persistent launch per pass shared by every transform) on one
-         stream and MsmBatch launches (every stage shared by up to 32 MSMs) on a second stream,
-         captured once into a CUDA graph and replayed.
+         stream and MsmBatch launches (every stage shared by up to 32 MSMs) over precomputed
+         resident tables on a second stream, captured once into a CUDA graph and replayed.
 """
 from __future__ import annotations
 
@@ -37,6 +40,8 @@ class MixedWorkload:
         self.ws = torch.empty(max(msm.workspace_size(1 << L, w) for L, w in zip(self.msm_logs, self.windows)),
                               dtype=torch.uint8, device=device)
         self.graph = None
+        self.tables = None
+        self.h_bases = None
 
     # ---- useful work, for throughput
     def work(self):
@@ -63,17 +68,67 @@ class MixedWorkload:
                                      1 << L, w, r.data_ptr(), torch.cuda.current_stream().cuda_stream
                                      if stream is None else stream.cuda_stream), "zkp_msm_device")
 
+    # ---- per-call path through the reference ABI (host arrays for the MSMs)
+    def run_plain_ref_abi(self, stream=None):
+        """Returns the MSM results (16 uint32 each, host); the NTTs transform ntt_bufs."""
+        for x, L, kind in zip(self.ntt_bufs, self.ntt_logs, self.ntt_kinds):
+            if kind == "ntt":
+                ntt.ssip_ntt(x, ntt.twiddle_table(L), stream)
+            elif kind == "intt":
+                ntt.ntt_ex(x, ntt.twiddle_table(L, True), None, ntt.n_inv(L), stream)
+            else:
+                ntt.ntt_ex(x, ntt.twiddle_table(L), ntt.scalar_const(7), None, stream)
+        if self.h_bases is None:
+            # host copies a runtime's host pool would hold (pinned)
+            self.h_bases = self.bases.cpu().pin_memory().numpy().view(np.uint32)
+            self.h_scalars = [s.cpu().pin_memory().numpy().view(np.uint32) for s in self.scalars]
+            n_max = 1 << max(self.msm_logs)
+            self.ref_ws = torch.empty(msm.MSM().get_buffer_size(n_max)[0], dtype=torch.uint8, device=self.device)
+        out = []
+        for hs, L in zip(self.h_scalars, self.msm_logs):
+            out.append(msm.msm_host_batches([hs], [self.h_bases[: 1 << L]], buffers=[self.ref_ws])[0])
+        return out
+
     # ---- batched path
+    def _resident_tables(self):
+        """Precomputed tables over the shared bases: one set per (window, table count) that the
+        resident configuration picks for the batch's sizes.  A task of n points reads the first
+        n rows of each table of its set (table_stride = the set's row count)."""
+        from .native import check, load
+        sets = {}
+        for L in self.msm_logs:
+            cfg = tuner.msm_resident_config(1 << L)
+            sets[cfg] = max(sets.get(cfg, 0), 1 << L)
+        lib = load(msm.LIB)
+        self.tables = {}
+        for (c, nt), rows in sets.items():
+            t = torch.empty((nt * rows, 16), dtype=torch.int32, device=self.device)
+            t[:rows].copy_(self.bases[:rows])
+            if nt > 1:
+                check(lib.zkp_msm_precompute_device(t.data_ptr(), rows, c, nt,
+                                                    torch.cuda.current_stream().cuda_stream),
+                      "zkp_msm_precompute_device")
+            self.tables[(c, nt)] = (t, rows)
+        torch.cuda.synchronize()
+
     def build_batched(self):
         self.ntt_batch = ntt.NttBatch(list(zip(self.ntt_bufs, self.ntt_kinds)))
-        tasks = [{"points": self.bases, "scalars": s, "n": 1 << L, "window": w, "result": r}
-                 for s, L, w, r in zip(self.scalars, self.msm_logs, self.windows, self.results)]
+        if self.tables is None:
+            self._resident_tables()
+        tasks = []
+        for s, L, r in zip(self.scalars, self.msm_logs, self.results):
+            c, nt = tuner.msm_resident_config(1 << L)
+            t, rows = self.tables[(c, nt)]
+            tasks.append({"points": t, "n_tables": nt, "table_stride": rows, "scalars": s, "n": 1 << L,
+                          "window": c, "result": r})
         self.msm_batches = [msm.MsmBatch(tasks[i:i + msm.MAX_BATCH]) for i in range(0, len(tasks), msm.MAX_BATCH)]
         self.s_main = torch.cuda.Stream()
         self.s_side = torch.cuda.Stream()
-        # warm the plans once outside capture
+        # warm the plans once outside capture (loads every kernel), then restore the inputs the
+        # warm-up transformed in place
         self._launch_batched()
         torch.cuda.synchronize()
+        self.reset_inputs()
         self.graph = torch.cuda.CUDAGraph()
         with torch.cuda.graph(self.graph, stream=self.s_main):
             self._launch_batched()

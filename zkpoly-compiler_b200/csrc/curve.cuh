@@ -5,7 +5,7 @@
 // points are (x, y) Montgomery Fq with (0, 0) the identity (PointAffine::is_identity tests
 // y == 0); an XYZZ point is the identity when zz == 0.
 //
-// Coordinates are lazy ([0, 2q)), so every "is zero" decision reduces modulo q first.
+// Coordinates are lazy ([0, 2q)), so every "is zero" decision is a test for 0 or q.
 #pragma once
 #include "field.cuh"
 
@@ -30,7 +30,7 @@ struct G1A {
         x.store(p);
         y.store(p + 8);
     }
-    ZK_DI bool is_identity() const { return y.canonical().is_zero(); }
+    ZK_DI bool is_identity() const { return y.is_zero_mod(); }
     ZK_DI G1A neg() const {
         G1A r;
         r.x = x;
@@ -59,7 +59,7 @@ struct G1X {
         r.zzz = Fq::one();
         return r;
     }
-    ZK_DI bool is_identity() const { return zz.canonical().is_zero(); }
+    ZK_DI bool is_identity() const { return zz.is_zero_mod(); }
 
     ZK_DI static G1X load(const u32 *p) {
         G1X r;
@@ -123,7 +123,7 @@ ZK_DI G1X g1_madd(const G1X &a, const G1A &b) {
     Fq s2 = Fq::mul(b.y, a.zzz);
     Fq p = Fq::sub(u2, a.x);
     Fq r = Fq::sub(s2, a.y);
-    if (p.canonical().is_zero() && r.canonical().is_zero()) return g1_dbl_affine(b);
+    if (p.is_zero_mod() && r.is_zero_mod()) return g1_dbl_affine(b);
     Fq pp = Fq::sqr(p);
     Fq ppp = Fq::mul(p, pp);
     Fq q = Fq::mul(a.x, pp);
@@ -145,7 +145,7 @@ ZK_DI G1X g1_add(const G1X &a, const G1X &b) {
     Fq s2 = Fq::mul(b.y, a.zzz);
     Fq p = Fq::sub(u2, u1);
     Fq r = Fq::sub(s2, s1);
-    if (p.canonical().is_zero() && r.canonical().is_zero()) return g1_dbl(a);
+    if (p.is_zero_mod() && r.is_zero_mod()) return g1_dbl(a);
     Fq pp = Fq::sqr(p);
     Fq ppp = Fq::mul(p, pp);
     Fq q = Fq::mul(u1, pp);
@@ -245,12 +245,13 @@ ZK_DI Fp<P> inv_binary(const Fp<P> &a_mont) {
         }
     }
     F r = bn_is_one(u) ? F::from_words(x1) : F::from_words(x2);
-    // r = (xR)^-1 = x^-1 R^-1; multiply by R^3 in Montgomery to get x^-1 R
+    // r = (xR)^-1 = x^-1 R^-1.  Each Montgomery product with R^2 multiplies by R:
+    // x^-1 R^-1 -> x^-1 -> x^-1 R (the Montgomery form of x^-1)
     F r2;
 #pragma unroll
     for (int i = 0; i < 8; i++) r2.v[i] = P::r2(i);
-    r = F::mul(r, r2);  // x^-1 R^-1 * R^2 * R^-1 = x^-1 R^0 ... times R below
-    r = F::mul(r, r2);  // x^-1 * R^2 * R^-1 = x^-1 R
+    r = F::mul(r, r2);
+    r = F::mul(r, r2);
     return r.canonical();
 }
 

@@ -299,7 +299,96 @@ struct Fp {
         t[8] = 0;
     }
 
-    ZK_DI static Fp sqr(const Fp &a) { return mul(a, a); }
+    // Montgomery square: the 28 off-diagonal products are formed once and doubled, the 8
+    // squares added, then the same word-serial reduction as mul (SOS order).  Each reduction
+    // row sees the same low word as the corresponding CIOS row of mul(a, a), so the quotient
+    // digits and therefore the lazy result are identical.
+    ZK_DI static Fp sqr(const Fp &a) {
+        u32 t[17];
+#pragma unroll
+        for (int i = 0; i < 17; i++) t[i] = 0;
+        // off-diagonal: t += a_i * a_j * 2^(32(i+j)) for i < j
+#pragma unroll
+        for (int i = 0; i < 7; i++) {
+            const u32 ai = a.v[i];
+            // low halves at positions i+j (j = i+1..7), carry into i+8
+            t[2 * i + 1] = mad_lo_cc(ai, a.v[i + 1], t[2 * i + 1]);
+#pragma unroll
+            for (int j = i + 2; j < 8; j++) t[i + j] = madc_lo_cc(ai, a.v[j], t[i + j]);
+            t[i + 8] = addc_cc(t[i + 8], 0u);
+            t[i + 9] = addc(t[i + 9], 0u);
+            // high halves at positions i+j+1, carry into i+9
+            t[2 * i + 2] = mad_hi_cc(ai, a.v[i + 1], t[2 * i + 2]);
+#pragma unroll
+            for (int j = i + 2; j < 8; j++) t[i + j + 1] = madc_hi_cc(ai, a.v[j], t[i + j + 1]);
+            t[i + 9] = addc(t[i + 9], 0u);
+        }
+        // double (t < 2^511 before, so no bit is lost)
+        t[16] = t[15] >> 31;
+#pragma unroll
+        for (int i = 15; i > 0; i--) t[i] = (t[i] << 1) | (t[i - 1] >> 31);
+        t[0] <<= 1;
+        // diagonal squares a_i^2 at positions 2i, 2i+1
+        t[0] = mad_lo_cc(a.v[0], a.v[0], t[0]);
+        t[1] = madc_hi_cc(a.v[0], a.v[0], t[1]);
+#pragma unroll
+        for (int i = 1; i < 8; i++) {
+            t[2 * i] = madc_lo_cc(a.v[i], a.v[i], t[2 * i]);
+            t[2 * i + 1] = madc_hi_cc(a.v[i], a.v[i], t[2 * i + 1]);
+        }
+        // word-serial Montgomery reduction of the 512-bit square.  Row i adds q*m at word i;
+        // the carries leaving its two chains at word i+8 are held in `pend` and added at word
+        // i+9 by the next row (a carry into a product word can itself overflow, so it is never
+        // dropped into a single addc).
+        u32 pend = 0;
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const u32 q = t[i] * P::MPRIME;
+            add_cc(t[i], 0xffffffffu);  // carry of t[i] + lo(q * m0), which is 0 mod 2^32
+            t[i + 1] = madc_lo_cc(q, P::m(1), t[i + 1]);
+            t[i + 2] = madc_lo_cc(q, P::m(2), t[i + 2]);
+            t[i + 3] = madc_lo_cc(q, P::m(3), t[i + 3]);
+            t[i + 4] = madc_lo_cc(q, P::m(4), t[i + 4]);
+            t[i + 5] = madc_lo_cc(q, P::m(5), t[i + 5]);
+            t[i + 6] = madc_lo_cc(q, P::m(6), t[i + 6]);
+            t[i + 7] = madc_lo_cc(q, P::m(7), t[i + 7]);
+            t[i + 8] = addc_cc(t[i + 8], pend);
+            const u32 c1 = addc(0u, 0u);
+            t[i + 1] = mad_hi_cc(q, P::m(0), t[i + 1]);
+            t[i + 2] = madc_hi_cc(q, P::m(1), t[i + 2]);
+            t[i + 3] = madc_hi_cc(q, P::m(2), t[i + 3]);
+            t[i + 4] = madc_hi_cc(q, P::m(3), t[i + 4]);
+            t[i + 5] = madc_hi_cc(q, P::m(4), t[i + 5]);
+            t[i + 6] = madc_hi_cc(q, P::m(5), t[i + 6]);
+            t[i + 7] = madc_hi_cc(q, P::m(6), t[i + 7]);
+            t[i + 8] = madc_hi_cc(q, P::m(7), t[i + 8]);
+            const u32 c2 = addc(0u, 0u);
+            pend = c1 + c2;
+            if (i < 7) {
+                // deliver the carries of this row at word i+9 before the next row reads it
+                t[i + 9] = add_cc(t[i + 9], pend);
+#pragma unroll
+                for (int k = i + 10; k < 16; k++) t[k] = addc_cc(t[k], 0u);
+                t[16] = addc(t[16], 0u);
+                pend = 0;
+            }
+        }
+        Fp r;
+#pragma unroll
+        for (int i = 0; i < 8; i++) r.v[i] = t[i + 8];
+        return r;
+    }
+
+    // x in [0, 2m) is 0 mod m exactly when x == 0 or x == m
+    ZK_DI bool is_zero_mod() const {
+        u32 z = 0, e = 0;
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            z |= v[i];
+            e |= v[i] ^ P::m(i);
+        }
+        return z == 0 || e == 0;
+    }
 
     // exponentiation by a 64-bit exponent (Element::pow with a small exponent)
     ZK_DI static Fp pow_u64(const Fp &a, u64 e) {

@@ -18,9 +18,10 @@
 //                walks its chunk with mixed additions.  Runs wholly inside a chunk are written
 //                straight to their bucket; runs cut by a chunk boundary leave partial sums that
 //                a fix-up pass joins.  Load balance does not depend on the scalar distribution.
-//   5. reduce:   per window sum_b b * S_b in parallel segments: each segment forms the running
-//                sums of its buckets (summation by parts) and adds (segment start) * segment
-//                sum; segments are then tree-summed.
+//   5. reduce:   per window sum_b b * S_b: short segments form their sums and running sums
+//                (summation by parts), the segment sums are split by the bits of their
+//                index into classes summed in parallel, and the classes are scaled by
+//                doublings and added.
 //   6. combine:  one thread folds the windows (c doublings each) and normalises to affine.
 #include <cuda_runtime.h>
 #include <dlfcn.h>
@@ -55,6 +56,8 @@ struct Task {
     u32 Wp;   // physical windows = ceil(W / n_tables)
     u32 B;    // buckets per window = 2^(c-1)
     u32 L;    // buckets per reduction segment
+    u32 gbits;  // log2(B / L): bit classes of the segment index
+    u32 parts;  // CTAs per class in the reduction
 };
 
 // The whole batch travels as a kernel parameter (no device copy, capturable in a graph).
@@ -68,6 +71,7 @@ struct Batch {
     u64 key_first[MAX_TASKS + 1];  // buckets (Wp * B per task)
     u64 seg_first[MAX_TASKS + 1];  // reduction segments (key count / L)
     u32 win_first[MAX_TASKS + 1];  // physical windows
+    u32 ncls, nparts;              // largest class count / parts of any task (reduction grid)
 };
 
 template <typename T>
@@ -89,7 +93,11 @@ inline Task make_task(u64 n, u32 c, u32 n_tables) {
     t.n_tables = n_tables;
     t.Wp = (t.W + n_tables - 1) / n_tables;
     t.B = 1u << (c - 1);
-    t.L = t.B < 16 ? t.B : 16;
+    t.L = t.B >= 8 ? 4 : t.B / 2;  // at least two segments per window
+    const u32 G = t.B / t.L;
+    t.gbits = 31 - __builtin_clz(G);
+    const u32 half = G / 2, per_cta = 256 * 8;  // about 8 additions per thread
+    t.parts = half / per_cta < 1 ? 1 : (half / per_cta > 8 ? 8 : half / per_cta);
     return t;
 }
 
@@ -113,6 +121,7 @@ inline u32 default_window(u64 n) {
 inline void finish_batch(Batch &b) {
     b.sc_first[0] = b.key_first[0] = b.seg_first[0] = 0;
     b.win_first[0] = 0;
+    b.ncls = b.nparts = 1;
     u64 entries = 0;
     for (u32 t = 0; t < b.ntasks; t++) {
         const Task &k = b.task[t];
@@ -120,6 +129,8 @@ inline void finish_batch(Batch &b) {
         b.key_first[t + 1] = b.key_first[t] + (u64)k.Wp * k.B;
         b.seg_first[t + 1] = b.seg_first[t] + (u64)k.Wp * k.B / k.L;
         b.win_first[t + 1] = b.win_first[t] + k.Wp;
+        b.ncls = b.ncls > k.gbits + 2 ? b.ncls : k.gbits + 2;
+        b.nparts = b.nparts > k.parts ? b.nparts : k.parts;
         entries += k.n * k.W;
     }
     // chunk so that roughly 4 waves of 384 threads per SM cover the entries
@@ -132,8 +143,8 @@ inline void finish_batch(Batch &b) {
 
 // ------------------------------------------------------------------ workspace layout
 struct Layout {
-    size_t counts, cursor, sorted_bucket, sorted_point, bucket_sums, part_pts, part_bucket, part_flag, seg, win,
-        total;
+    size_t counts, cursor, sorted_bucket, sorted_point, bucket_sums, part_pts, part_bucket, part_flag, long_list,
+        seg, cls, win, total;
     u64 nb, entries, chunks, segs, wins;
 };
 
@@ -161,7 +172,9 @@ inline Layout make_layout(const Batch &b) {
     l.part_pts = take(l.chunks * 2 * 128);
     l.part_bucket = take(l.chunks * 2 * 4);
     l.part_flag = take(l.chunks * 2 * 4);
-    l.seg = take(l.segs * 128);
+    l.long_list = take((l.chunks + 1) * 4 + 4);  // chain starts + a counter at the end
+    l.seg = take(2 * l.segs * 128);  // U_g then T_g
+    l.cls = take(l.wins * b.ncls * b.nparts * 128);
     l.win = take(l.wins * 128);
     l.total = off;
     return l;
@@ -341,9 +354,10 @@ ZK_DI G1A fetch_point(const u32 *points, u32 code) {
 // the previous chunk, ends here), 2 = head run that also continues into the next chunk,
 // 3 = tail run (starts here, continues into the next).  Buckets of different tasks never
 // share a key, so runs never span two tasks.
-__global__ void __launch_bounds__(256) accumulate_kernel(const Batch b, const u32 *sorted_bucket,
-                                                        const u32 *sorted_point, const u32 *live, u32 *bucket_sums,
-                                                        u32 *part_pts, u32 *part_bucket, u32 *part_flag) {
+__global__ void __launch_bounds__(256, 2) accumulate_kernel(const Batch b, const u32 *sorted_bucket,
+                                                           const u32 *sorted_point, const u32 *live,
+                                                           u32 *bucket_sums, u32 *part_pts, u32 *part_bucket,
+                                                           u32 *part_flag) {
     const u64 entries = *live;
     const u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x;
     const u64 start = t * b.K;
@@ -354,10 +368,32 @@ __global__ void __launch_bounds__(256) accumulate_kernel(const Batch b, const u3
     u32 cur = sorted_bucket[start];
     const u32 *pts = b.task[find_task(b.key_first, b.ntasks, (u64)cur)].points;
     G1X acc = G1X::from_affine(fetch_point(pts, sorted_point[start]));
+    // The point of the next entry is always in flight while the current one is added: its
+    // load is issued one iteration ahead and its sign applied only when it is used.
+    u32 nbk = EMPTY, ncode = 0;
+    const u32 *npts = pts;
+    G1A nxt;
+    if (start + 1 < end) {
+        nbk = sorted_bucket[start + 1];
+        ncode = sorted_point[start + 1];
+        if (nbk != cur) npts = b.task[find_task(b.key_first, b.ntasks, (u64)nbk)].points;
+        nxt = G1A::load_nc(npts + (u64)(ncode & 0x7fffffffu) * 16);
+    }
     for (u64 p = start + 1; p <= end; p++) {
-        const u32 bk = p < end ? sorted_bucket[p] : EMPTY;
+        const u32 bk = nbk, code = ncode;
+        const u32 *bpts = npts;
+        G1A pt = nxt;
+        if (p + 1 < end) {
+            nbk = sorted_bucket[p + 1];
+            ncode = sorted_point[p + 1];
+            if (nbk != bk) npts = b.task[find_task(b.key_first, b.ntasks, (u64)nbk)].points;
+            nxt = G1A::load_nc(npts + (u64)(ncode & 0x7fffffffu) * 16);
+        } else {
+            nbk = EMPTY;
+        }
+        if (p < end && (code & 0x80000000u)) pt = pt.neg();
         if (p < end && bk == cur) {
-            acc = g1_madd(acc, fetch_point(pts, sorted_point[p]));
+            acc = g1_madd(acc, pt);
             continue;
         }
         const bool head = run_start == start && from_prev;
@@ -373,62 +409,112 @@ __global__ void __launch_bounds__(256) accumulate_kernel(const Batch b, const u3
         if (p < end) {
             cur = bk;
             run_start = p;
-            pts = b.task[find_task(b.key_first, b.ntasks, (u64)cur)].points;
-            acc = G1X::from_affine(fetch_point(pts, sorted_point[p]));
+            pts = bpts;
+            acc = G1X::from_affine(pt);
         }
     }
 }
 
-// joins the partial sums of every run that crosses chunk boundaries
+// Joins the partial sums of every run that crosses chunk boundaries.  A run's partials sit in
+// consecutive chunks: the tail slot of its first chunk t0, then the head slots of the chunks
+// after it.  One thread joins a short run; a run longer than SHORT_CHAIN chunks (a huge bucket:
+// equal scalars, or a top window with very few bits) is handed to long_chain_kernel, where a
+// whole CTA reduces it in parallel.
+constexpr u32 SHORT_CHAIN = 32;
+
+ZK_DI bool chain_member(const u32 *part_bucket, const u32 *part_flag, u64 u, u32 bucket) {
+    const u32 f = part_flag[2 * u];
+    return (f == 1u || f == 2u) && part_bucket[2 * u] == bucket;
+}
+
 __global__ void __launch_bounds__(256) fixup_kernel(const u32 *live, u32 K, u32 *bucket_sums, const u32 *part_pts,
-                                                   const u32 *part_bucket, const u32 *part_flag) {
+                                                   const u32 *part_bucket, const u32 *part_flag, u32 *long_list,
+                                                   u32 *long_count) {
     const u64 chunks = ((u64)*live + K - 1) / K;
     const u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= chunks || part_flag[2 * t + 1] != 3u) return;
     const u64 slot = 2 * t + 1;
     const u32 bucket = part_bucket[slot];
+    // a chain longer than SHORT_CHAIN goes to the CTA-wide pass
+    const u64 probe = t + 1 + SHORT_CHAIN;
+    if (probe < chunks && chain_member(part_bucket, part_flag, probe - 1, bucket) &&
+        part_flag[2 * (probe - 1)] == 2u) {
+        long_list[atomicAdd(long_count, 1u)] = (u32)t;
+        return;
+    }
     G1X acc = G1X::load(part_pts + slot * 32);
     for (u64 u = t + 1; u < chunks; u++) {
-        const u32 f = part_flag[2 * u];
-        if ((f != 1u && f != 2u) || part_bucket[2 * u] != bucket) break;
+        if (!chain_member(part_bucket, part_flag, u, bucket)) break;
         acc = g1_add(acc, G1X::load(part_pts + 2 * u * 32));
-        if (f == 1u) break;
+        if (part_flag[2 * u] == 1u) break;
     }
     acc.store(bucket_sums + (u64)bucket * 32);
 }
 
+// one CTA per long chain (looping over the recorded list): strided partial sums, then a tree
+__global__ void __launch_bounds__(128) long_chain_kernel(const u32 *live, u32 K, u32 *bucket_sums,
+                                                        const u32 *part_pts, const u32 *part_bucket,
+                                                        const u32 *part_flag, const u32 *long_list,
+                                                        const u32 *long_count) {
+    __shared__ u32 sm[128 * 32];
+    const u64 chunks = ((u64)*live + K - 1) / K;
+    const u32 nlong = *long_count;
+    for (u32 item = blockIdx.x; item < nlong; item += gridDim.x) {
+        const u64 t0 = long_list[item];
+        const u32 bucket = part_bucket[2 * t0 + 1];
+        G1X acc = threadIdx.x == 0 ? G1X::load(part_pts + (2 * t0 + 1) * 32) : G1X::identity();
+        // members are the contiguous chunks t0+1 .. t1; each thread takes every blockDim-th
+        for (u64 u = t0 + 1 + threadIdx.x; u < chunks; u += blockDim.x) {
+            if (!chain_member(part_bucket, part_flag, u, bucket)) break;
+            // a flag-1 head ends the chain, but threads strided past it stop at the next
+            // non-member anyway; a member after an earlier flag-1 end cannot share the bucket id
+            // because bucket ids are strictly increasing along the sorted array
+            acc = g1_add(acc, G1X::load(part_pts + 2 * u * 32));
+        }
+        acc.store(sm + threadIdx.x * 32);
+        __syncthreads();
+        for (u32 stride = blockDim.x / 2; stride > 0; stride >>= 1) {
+            if (threadIdx.x < stride) {
+                G1X a = G1X::load(sm + threadIdx.x * 32);
+                G1X b = G1X::load(sm + (threadIdx.x + stride) * 32);
+                g1_add(a, b).store(sm + threadIdx.x * 32);
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) G1X::load(sm).store(bucket_sums + (u64)bucket * 32);
+        __syncthreads();
+    }
+}
+
 // ------------------------------------------------------------------ 5: bucket reduction
-// global segment s of task t covers buckets key_first[t] + s_l*L .. + L - 1; with g the
-// segment's index inside its window, it yields
-//   sum_j (g*L + j + 1) * S_j = (running sums of the segment) + (g*L) * (segment sum)
-__global__ void __launch_bounds__(128) segment_kernel(const Batch b, const u32 *bucket_sums, u32 *seg_out) {
+// A physical window's value is sum_j (j + 1) S_j over its B buckets.  With segments of L
+// buckets (g < G = B / L), U_g = the segment's sum and T_g = sum_i (i + 1) S_{gL+i}, the value
+// is  sum_g T_g + L * sum_g g U_g,  and  sum_g g U_g = sum_k 2^k X_k  with X_k the sum of the
+// U_g whose index g has bit k set.  segment_kernel forms U_g and T_g (2L additions per
+// thread); class_kernel sums every class (each X_k, and the T_g in two halves) in parallel
+// parts; window_kernel joins the parts, scales X_k by 2^k * L with doublings and adds the
+// classes.  Every chain of dependent additions stays short, so a window of 2^16 buckets is
+// reduced by tens of thousands of threads instead of a few thousand long ones.
+__global__ void __launch_bounds__(128) segment_kernel(const Batch b, const u32 *bucket_sums, u32 *seg_u,
+                                                     u32 *seg_t) {
     const u64 s = (u64)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= b.seg_first[b.ntasks]) return;
     const u32 t = find_task(b.seg_first, b.ntasks, s);
     const Task &k = b.task[t];
     const u64 sl = s - b.seg_first[t];
-    const u64 g = sl % (k.B / k.L);
     const u32 *base = bucket_sums + (b.key_first[t] + sl * k.L) * 32;
     G1X run = G1X::identity(), acc = G1X::identity();
     for (int j = (int)k.L - 1; j >= 0; j--) {
         run = g1_add(run, G1X::load(base + (u64)j * 32));
         acc = g1_add(acc, run);
     }
-    if (g > 0) acc = g1_add(acc, g1_mul_u64(run, g * k.L));
-    acc.store(seg_out + s * 32);
+    run.store(seg_u + s * 32);
+    acc.store(seg_t + s * 32);
 }
 
-// per physical window (one CTA each): tree-sum of its segments
-__global__ void __launch_bounds__(256) window_sum_kernel(const Batch b, const u32 *seg_out, u32 *win_out) {
-    __shared__ u32 sm[256 * 32];
-    const u32 wg = blockIdx.x;
-    const u32 t = find_task(b.win_first, b.ntasks, wg);
-    const Task &k = b.task[t];
-    const u64 spw = k.B / k.L;
-    const u32 *base = seg_out + (b.seg_first[t] + (u64)(wg - b.win_first[t]) * spw) * 32;
-    G1X acc = G1X::identity();
-    for (u64 i = threadIdx.x; i < spw; i += blockDim.x) acc = g1_add(acc, G1X::load(base + i * 32));
-    acc.store(sm + threadIdx.x * 32);
+// sum of the CTA's per-thread points (256 threads) into sm[0]
+ZK_DI void cta_tree_sum(u32 *sm, const G1X &mine) {
+    mine.store(sm + threadIdx.x * 32);
     __syncthreads();
     for (u32 stride = blockDim.x / 2; stride > 0; stride >>= 1) {
         if (threadIdx.x < stride) {
@@ -438,7 +524,64 @@ __global__ void __launch_bounds__(256) window_sum_kernel(const Batch b, const u3
         }
         __syncthreads();
     }
-    if (threadIdx.x == 0) G1X::load(sm).store(win_out + (u64)wg * 32);
+}
+
+// grid (windows, classes, parts): class k < gbits sums U_g over the g with bit k set; classes
+// gbits and gbits + 1 sum T_g over the lower and upper half of g.  Each class has G/2 items,
+// split into `parts` equal ranges, one CTA each.
+__global__ void __launch_bounds__(256) class_kernel(const Batch b, const u32 *seg_u, const u32 *seg_t,
+                                                   u32 *cls_out) {
+    __shared__ u32 sm[256 * 32];
+    const u32 wg = blockIdx.x, cls = blockIdx.y, part = blockIdx.z;
+    const u32 t = find_task(b.win_first, b.ntasks, wg);
+    const Task &k = b.task[t];
+    if (cls >= k.gbits + 2 || part >= k.parts) return;  // the whole CTA leaves together
+    const u64 G = k.B / k.L, half = G / 2;
+    const u64 seg0 = b.seg_first[t] + (u64)(wg - b.win_first[t]) * G;
+    const u64 per = half / k.parts;
+    const u64 m0 = (u64)part * per;
+    const bool is_t = cls >= k.gbits;
+    const u32 *src = is_t ? seg_t : seg_u;
+    G1X acc = G1X::identity();
+    for (u64 m = m0 + threadIdx.x; m < m0 + per; m += blockDim.x) {
+        const u64 g = is_t ? m + (u64)(cls - k.gbits) * half
+                           : ((m >> cls) << (cls + 1)) | (1ull << cls) | (m & ((1ull << cls) - 1));
+        acc = g1_add(acc, G1X::load(src + (seg0 + g) * 32));
+    }
+    cta_tree_sum(sm, acc);
+    if (threadIdx.x == 0) G1X::load(sm).store(cls_out + (((u64)wg * b.ncls + cls) * b.nparts + part) * 32);
+}
+
+// one CTA (256 threads) per physical window: parts -> classes -> 2^k L X_k -> window value
+__global__ void __launch_bounds__(256) window_kernel(const Batch b, const u32 *cls_out, u32 *win_out) {
+    __shared__ u32 sm[256 * 32];
+    const u32 wg = blockIdx.x;
+    const u32 t = find_task(b.win_first, b.ntasks, wg);
+    const Task &k = b.task[t];
+    const u32 ncls = k.gbits + 2, P = k.parts, tid = threadIdx.x;
+    G1X v = G1X::identity();
+    if (tid < ncls * P) v = G1X::load(cls_out + (((u64)wg * b.ncls + tid / P) * b.nparts + tid % P) * 32);
+    v.store(sm + tid * 32);
+    __syncthreads();
+    for (u32 st = P / 2; st > 0; st >>= 1) {  // the parts of each class, P a power of two
+        if (tid < ncls * P && (tid % P) < st) {
+            G1X x = G1X::load(sm + tid * 32);
+            G1X y = G1X::load(sm + (tid + st) * 32);
+            g1_add(x, y).store(sm + tid * 32);
+        }
+        __syncthreads();
+    }
+    G1X x = G1X::identity();
+    if (tid < ncls) {
+        x = G1X::load(sm + tid * P * 32);
+        if (tid < k.gbits) {
+            const u32 dbls = tid + (31 - __clz(k.L));  // 2^tid * L
+            for (u32 i = 0; i < dbls; i++) x = g1_dbl(x);
+        }
+    }
+    __syncthreads();
+    cta_tree_sum(sm, x);
+    if (tid == 0) G1X::load(sm).store(win_out + (u64)wg * 32);
 }
 
 // ------------------------------------------------------------------ 6: window combination
@@ -497,7 +640,10 @@ cudaError_t run_batch(const Batch &b, const Layout &l, char *ws, cudaStream_t st
     u32 *pp = reinterpret_cast<u32 *>(ws + l.part_pts);
     u32 *pb = reinterpret_cast<u32 *>(ws + l.part_bucket);
     u32 *pf = reinterpret_cast<u32 *>(ws + l.part_flag);
+    u32 *longs = reinterpret_cast<u32 *>(ws + l.long_list);
+    u32 *nlong = longs + l.chunks + 1;
     u32 *seg = reinterpret_cast<u32 *>(ws + l.seg);
+    u32 *cls = reinterpret_cast<u32 *>(ws + l.cls);
     u32 *win = reinterpret_cast<u32 *>(ws + l.win);
     const u64 nb = l.nb;
 
@@ -506,6 +652,7 @@ cudaError_t run_batch(const Batch &b, const Layout &l, char *ws, cudaStream_t st
     ZK_TRY(cudaMemsetAsync(counts, 0, (nb + 1) * 4, stream));
     ZK_TRY(cudaMemsetAsync(bs, 0, nb * 128, stream));
     ZK_TRY(cudaMemsetAsync(pf, 0, l.chunks * 2 * 4, stream));
+    ZK_TRY(cudaMemsetAsync(nlong, 0, 4, stream));
     prof.mark("memset", stream);
     const u64 scalars = b.sc_first[b.ntasks];
     if (scalars) {
@@ -535,17 +682,22 @@ cudaError_t run_batch(const Batch &b, const Layout &l, char *ws, cudaStream_t st
     }
     prof.mark("accumulate", stream);
     if (l.chunks) {
-        fixup_kernel<<<(u32)((l.chunks + 255) / 256), 256, 0, stream>>>(live, b.K, bs, pp, pb, pf);
+        fixup_kernel<<<(u32)((l.chunks + 255) / 256), 256, 0, stream>>>(live, b.K, bs, pp, pb, pf, longs, nlong);
+        ZK_TRY(cudaGetLastError());
+        long_chain_kernel<<<num_sms() * 2, 128, 0, stream>>>(live, b.K, bs, pp, pb, pf, longs, nlong);
         ZK_TRY(cudaGetLastError());
     }
     prof.mark("fixup", stream);
     if (l.segs) {
-        segment_kernel<<<(u32)((l.segs + 127) / 128), 128, 0, stream>>>(b, bs, seg);
+        segment_kernel<<<(u32)((l.segs + 127) / 128), 128, 0, stream>>>(b, bs, seg, seg + l.segs * 32);
         ZK_TRY(cudaGetLastError());
     }
     prof.mark("segment", stream);
     if (l.wins) {
-        window_sum_kernel<<<(u32)l.wins, 256, 0, stream>>>(b, seg, win);
+        class_kernel<<<dim3((u32)l.wins, b.ncls, b.nparts), 256, 0, stream>>>(b, seg, seg + l.segs * 32, cls);
+        ZK_TRY(cudaGetLastError());
+        prof.mark("classes", stream);
+        window_kernel<<<(u32)l.wins, 256, 0, stream>>>(b, cls, win);
         ZK_TRY(cudaGetLastError());
     }
     prof.mark("window_sum", stream);

@@ -319,15 +319,26 @@ struct Plan {
     u32 lo[4];
 };
 
+// Per-size cap on the digit width (the sub-transform size 2^D of a pass), set by the tuner
+// through zkp_ntt_set_max_digit; 0 means MAX_D.  A smaller cap means more passes but smaller
+// CTAs, several of which share an SM (one loads or stores while another computes).
+std::atomic<u32> g_max_digit[29];
+
+inline u32 digit_cap(u32 L) {
+    const u32 d = L < 29 ? g_max_digit[L].load(std::memory_order_relaxed) : 0;
+    return d ? d : MAX_D;
+}
+
 inline Plan make_plan(u32 L) {
     Plan p{};
-    if (L <= MAX_D) {
+    const u32 cap = digit_cap(L);
+    if (L <= cap) {
         p.np = 1;
         p.D[0] = L;
         p.lo[0] = 0;
         return p;
     }
-    p.np = (L + MAX_D - 1) / MAX_D;
+    p.np = (L + cap - 1) / cap;
     u32 base = L / p.np, extra = L % p.np;
     u32 rem = L;
     for (u32 i = 0; i < p.np; i++) {
@@ -609,6 +620,16 @@ extern "C" void zkp_ntt_batch_plan_destroy(ZkpNttBatchPlan *plan) {
     cudaFree(plan->mem);
     cudaSetDevice(prev);
     delete plan;
+}
+
+extern "C" cudaError_t zkp_ntt_set_max_digit(unsigned int log_len, unsigned int max_digit) {
+    ZK_CHECK_ARG(log_len <= 28 && (max_digit == 0 || (max_digit >= 4 && max_digit <= ntt::MAX_D)));
+    if (log_len == 0) {
+        for (u32 L = 0; L < 29; L++) ntt::g_max_digit[L].store(max_digit);
+    } else {
+        ntt::g_max_digit[log_len].store(max_digit);
+    }
+    return cudaSuccess;
 }
 
 extern "C" unsigned int zkp_ntt_num_passes(unsigned int log_len) {

@@ -40,7 +40,7 @@ inline View plain_view(void *p, u64 n) {
 }
 
 // ------------------------------------------------------------------ elementwise
-enum Op : u32 { OP_ADD = 0, OP_SUB = 1, OP_MUL = 2, OP_SUBR = 3 };
+enum Op : u32 { OP_ADD = 0, OP_SUB = 1, OP_MUL = 2, OP_SUBR = 3, OP_SQR = 4 };
 
 // dst[i] = a[i] op b[i] for i < len; dst[i] = a[i] (or -a[i] for reversed subtraction) for
 // len <= i < upper (poly_basic.cuh:4-65: the longer operand passes through)
@@ -54,6 +54,7 @@ __global__ void __launch_bounds__(256) binary_kernel(View dst, View a, View b, u
                 case OP_ADD: r = Fr::add_c(x, y); break;
                 case OP_SUB: r = Fr::sub_c(x, y); break;
                 case OP_SUBR: r = Fr::sub_c(y, x); break;
+                case OP_SQR: r = Fr::sqr(x).canonical(); break;
                 default: r = Fr::mul(x, y).canonical(); break;
             }
         } else {
@@ -300,6 +301,9 @@ extern "C" cudaError_t poly_sub(PolyPtr r, ConstPolyPtr a, ConstPolyPtr b, cudaS
 }
 extern "C" cudaError_t poly_mul(PolyPtr r, ConstPolyPtr a, ConstPolyPtr b, cudaStream_t stream) {
     return binary_op(r, a, b, OP_MUL, stream);
+}
+extern "C" cudaError_t zkp_poly_square(PolyPtr r, ConstPolyPtr a, cudaStream_t stream) {
+    return binary_op(r, a, a, OP_SQR, stream);
 }
 
 static cudaError_t fill(PolyPtr t, u32 kind, bool coef, cudaStream_t stream) {

@@ -22,9 +22,18 @@ from .scalar import ScalarArray, device_words, require_cuda, stream_handle
 LIB = "libntt.so"
 
 
+_plans_applied = False
+
+
 def _lib():
+    global _plans_applied
     require_cuda()
-    return load(LIB)
+    lib = load(LIB)
+    if not _plans_applied:
+        _plans_applied = True
+        from . import tuner
+        tuner.apply_ntt_plans()  # tuned digit caps for this GPU model, if cached
+    return lib
 
 
 def _ptr(t: torch.Tensor | None) -> int | None:

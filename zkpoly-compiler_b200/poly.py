@@ -44,6 +44,10 @@ def poly_mul(r: ScalarArray, a: ScalarArray, b: ScalarArray, stream=None):
     check(_lib().poly_mul(r.poly_ptr(), a.poly_ptr(), b.poly_ptr(), stream_handle(stream)), "poly_mul")
 
 
+def poly_square(r: ScalarArray, a: ScalarArray, stream=None):
+    check(_lib().zkp_poly_square(r.poly_ptr(), a.poly_ptr(), stream_handle(stream)), "zkp_poly_square")
+
+
 def poly_one_lagrange(t: ScalarArray, stream=None):
     check(_lib().poly_one_lagrange(t.poly_ptr(), stream_handle(stream)), "poly_one_lagrange")
 

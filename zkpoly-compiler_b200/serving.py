@@ -66,6 +66,109 @@ class Server:
         self.close()
 
 
+class PerCallProver:
+    """The plain per-call path: the served program (include/zkp_runtime.h), one request at a
+    time, every operator called through its own per-call entry point on one stream.  The four
+    MSMs go through the reference ABI `msm` (core/src/msm.rs:302-369): the runtime hands that
+    call host scalar arrays and host point tables and gets host affine results back, so each
+    request moves its MSM inputs device -> host -> device, as the reference's runtime does.
+    Results are bit-identical to the served form's (the test suite checks it)."""
+
+    def __init__(self, bases, ext_log: int = 2, device="cuda", max_k: int | None = None):
+        from . import msm
+        require_cuda()
+        pts = bases.tables[: bases.n] if hasattr(bases, "tables") else bases
+        # host point table (pinned, as a runtime's host pool would hand it out)
+        self.h_bases = pts.cpu().pin_memory()
+        self.h_bases_np = self.h_bases.numpy().view(np.uint32)
+        self.ext = ext_log
+        self.device = device
+        self.cfg = msm.MsmConfig()
+        self._ws = None
+        self._stage = None
+        if max_k is not None:  # the pinned staging area up front, outside any timed loop
+            self._stage = torch.empty((4, 1 << max_k, 8), dtype=torch.int32).pin_memory()
+        self._consts = {}
+
+    def _const(self, k: int):
+        from . import fused, ntt, pipeline
+        if k not in self._consts:
+            self._consts[k] = {
+                "inv_tw": ntt.twiddle_table(k, True, self.device),
+                "fwd_tw": ntt.twiddle_table(k + self.ext, False, self.device),
+                "ninv": ntt.n_inv(k, self.device),
+                "shift": ntt.scalar_const(pipeline.SHIFT, self.device),
+                "zh": pipeline.zh_inv_device(k, self.ext, self.device),
+            }
+            if not hasattr(self, "quotient"):
+                self.quotient = fused.quotient_kernel()
+        return self._consts[k]
+
+    def warm(self, ks) -> None:
+        """Builds the per-size constants (root tables, n^-1, 1/Z_H) ahead of time, as the
+        served form does when it is created."""
+        for k in ks:
+            self._const(k)
+        torch.cuda.synchronize()
+
+    def run(self, k: int, seed: int) -> np.ndarray:
+        """Result words (4 MSM points, 2 evaluations) of request (k, seed), as result_words."""
+        from . import gen, msm, ntt, pipeline, poly
+        from .scalar import ScalarArray
+        c = self._const(k)
+        n, N = 1 << k, 1 << (k + self.ext)
+        s = seed * 8
+        a, b, cc = (ScalarArray(gen.fr(s + i, n, self.device)) for i in range(3))
+        z = ScalarArray(gen.fr(s + 3, N, self.device))
+        x = gen.fr(s + 4, 1, self.device)
+        for v in (a, b, cc):
+            ntt.ntt_ex(v, c["inv_tw"], None, c["ninv"])
+        e = ScalarArray.alloc(N, self.device)
+        ntt.coset_lde(e, cc, c["fwd_tw"], c["shift"])
+        q = ScalarArray.alloc(N, self.device)
+        self.quotient([q], [e, e, e, z, pipeline.rotated(z, self.ext), c["zh"]])
+        # reference-ABI MSM: host scalars in (staged in pinned memory, as a runtime's host pool
+        # would hold them), host affine points out
+        if self._stage is None or self._stage.shape[1] < n:
+            self._stage = torch.empty((4, n, 8), dtype=torch.int32).pin_memory()
+        for i, t in enumerate((a, b, cc, q)):
+            self._stage[i, :n].copy_(t.values[:n])
+        stage = self._stage.numpy().view(np.uint32)
+        host_scalars = [stage[i, :n] for i in range(4)]
+        sizes = msm.MSM(self.cfg).get_buffer_size(n)
+        if self._ws is None or self._ws.numel() < sizes[0]:
+            self._ws = torch.empty(sizes[0], dtype=torch.uint8, device=self.device)
+        points = msm.msm_host_batches(host_scalars, [self.h_bases_np[:n]], buffers=[self._ws], cfg=self.cfg)
+        ev = torch.zeros((2, 8), dtype=torch.int32, device=self.device)
+        poly.poly_eval(a, x, ev[0])
+        poly.poly_eval(b, x, ev[1])
+        return np.concatenate([p.view(np.uint32) for p in points] + [ev.cpu().numpy().view(np.uint32).ravel()])
+
+
+def run_schedule_per_call(prover: PerCallProver, schedule):
+    """The plain path under the same arrivals: requests run one after another in arrival
+    order; latency = completion - arrival (host clock)."""
+    start = time.perf_counter()
+    lat, words = [], []
+    first = last = None
+    for t_arr, k, seed in schedule:
+        delay = t_arr - (time.perf_counter() - start)
+        if delay > 0:
+            time.sleep(delay)
+        t0 = time.perf_counter()
+        words.append(prover.run(k, seed))
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        first = t0 if first is None else first
+        last = t1
+        lat.append((t1 - start - t_arr) * 1e3)
+    lat = np.array(lat)
+    summary = {"requests": len(schedule), "ok": len(schedule), "p50_ms": float(np.percentile(lat, 50)),
+               "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()),
+               "req_per_s": len(schedule) / (last - start - schedule[0][0])}
+    return words, summary
+
+
 def result_words(res: ZkpProverResult) -> np.ndarray:
     """msm points and evals of a result as one uint32 vector (for bit-exact comparisons)."""
     return np.concatenate([np.frombuffer(bytes(res.msm), dtype=np.uint32),

@@ -6,8 +6,9 @@ Tuned parameters:
   - MSM window width c in [8, 20] per log2 n (zkp_msm_device timed on seeded inputs);
   - NTT largest digit (sub-transform size 2^D, which sets the pass split and the CTA shape)
     per log2 n (zkp_ntt_set_max_digit, timed on seeded inputs).
-The cache is a JSON file next to the libraries; without an entry the libraries' own cost
-model / default plan is used.
+The cache is a JSON file next to the libraries.  Below it sit the shipped defaults
+(tuning_defaults.json, winners this tuner measured on B200); without an entry in either the
+libraries' own cost model / default plan is used.
 """
 from __future__ import annotations
 
@@ -21,6 +22,7 @@ from .native import check, load
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CACHE = os.path.join(HERE, "lib", "tuning.json")
+DEFAULTS = os.path.join(HERE, "tuning_defaults.json")
 _lock = threading.Lock()
 _cache: dict | None = None
 
@@ -32,11 +34,16 @@ def _device_key() -> str:
 def _load() -> dict:
     global _cache
     if _cache is None:
-        try:
-            with open(CACHE) as f:
-                _cache = json.load(f)
-        except (OSError, ValueError):
-            _cache = {}
+        _cache = {}
+        for path in (DEFAULTS, CACHE):  # measured entries override the shipped ones
+            try:
+                with open(path) as f:
+                    data = json.load(f)
+            except (OSError, ValueError):
+                continue
+            for dev, kinds in data.items():
+                for kind, table in kinds.items():
+                    _cache.setdefault(dev, {}).setdefault(kind, {}).update(table)
     return _cache
 
 
@@ -62,8 +69,15 @@ def msm_resident_config(n: int):
     entry = _load().get(_device_key(), {}).get("msm_resident", {}).get(str(log_n))
     if entry:
         return int(entry[0]), int(entry[1])
-    c = 16
+    c = resident_window_model(1 << log_n)
     return c, (254 + c - 1) // c
+
+
+def resident_window_model(n: int) -> int:
+    """Untuned window for full precomputation: minimises n * ceil(254 / c) bucket additions
+    plus a bucket-reduction cost of 40 * 2^c (in the same unit, fitted to B200 timings at
+    n = 2^22 where it picks c = 17)."""
+    return min(range(8, 21), key=lambda c: n * ((254 + c - 1) // c) + 40 * (1 << c))
 
 
 def _time(fn, reps=3) -> float:
@@ -104,6 +118,43 @@ def tune_msm(log_ns=range(12, 23), candidates=range(8, 21), bases=None) -> dict:
         _load().setdefault(_device_key(), {})["msm_window"] = out
         _save()
     return out
+
+
+def tune_ntt(log_ns=range(14, 25), candidates=(8, 9, 10, 11, 12), apply: bool = True) -> dict:
+    """Times a forward NTT of 2^L seeded elements for each digit cap (zkp_ntt_set_max_digit)
+    and caches the fastest per size; with apply the winners are set in the library."""
+    from . import gen, ntt
+    from .scalar import ScalarArray
+    lib = load(ntt.LIB)
+    out, times = {}, {}
+    for L in log_ns:
+        x = ScalarArray(gen.fr(79, 1 << L))
+        tw = ntt.twiddle_table(L)
+        best = None
+        for d in candidates:
+            check(lib.zkp_ntt_set_max_digit(L, d), "zkp_ntt_set_max_digit")
+            t = _time(lambda: ntt.ssip_ntt(x, tw), reps=3)
+            times[f"{L}:{d}"] = t
+            if best is None or t < best[1]:
+                best = (d, t)
+        check(lib.zkp_ntt_set_max_digit(L, 0), "zkp_ntt_set_max_digit")
+        out[str(L)] = best[0]
+        del x
+    with _lock:
+        _load().setdefault(_device_key(), {})["ntt_max_digit"] = out
+        _save()
+    if apply:
+        apply_ntt_plans()
+    return {"best": out, "ms": times}
+
+
+def apply_ntt_plans() -> None:
+    """Sets the cached digit caps (if any) for this GPU model in libntt.so."""
+    from . import ntt
+    table = _load().get(_device_key(), {}).get("ntt_max_digit", {})
+    lib = load(ntt.LIB)
+    for L, d in table.items():
+        check(lib.zkp_ntt_set_max_digit(int(L), int(d)), "zkp_ntt_set_max_digit")
 
 
 def tune_msm_resident(log_n: int = 22, windows=(13, 14, 15, 16, 17, 18, 19, 20), full_only: bool = True,
