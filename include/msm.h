@@ -82,6 +82,25 @@ cudaError_t zkp_msm_batch(const ZkpMsmTask *tasks, unsigned int ntasks, void *wo
 cudaError_t zkp_msm_precompute_device(unsigned int *tables_d, unsigned long long n, unsigned int window,
                                       unsigned int n_tables, cudaStream_t stream);
 
+/* ---- allocation-free MSM (no counterpart in the reference) ----
+ * For callers that cannot allocate device memory - a plugin whose host application only hands
+ * it input and output buffers and owns every allocator, or a latency-critical loop that must
+ * not call cudaMalloc because it synchronises the whole device.  Same result as
+ * zkp_msm_device, but the workspace is a fixed 64 MiB array inside the library (every GPU that
+ * loads the library holds it until the process exits), which fits MSMs of up to 2^15 points
+ * with the default window (2^16 points need 68.8 MiB); larger problems return
+ * cudaErrorInvalidValue without touching the device.  The call allocates nothing.  Nothing in
+ * the array has to start at zero: each call clears the counters, bucket sums and flags it uses,
+ * on its stream, before its kernels read them.  Its first call on a device looks up that
+ * device's copy of the array, so make that first call before any stream capture.  Every call
+ * shares the one array, which keeps the last call's contents: calls that overlap on the GPU
+ * (other streams, other host threads) race, so serialise them on one stream. */
+cudaError_t zkp_msm_device_noalloc(const unsigned int *points_d, unsigned int n_tables,
+                                   const unsigned int *scalars_d, unsigned long long n, unsigned int window,
+                                   unsigned int *result_d, cudaStream_t stream);
+/* Bytes of the fixed workspace zkp_msm_device_noalloc uses (compare zkp_msm_workspace_size). */
+unsigned long long zkp_msm_noalloc_capacity(void);
+
 /* Benchmark support: per-stage CUDA-event timing of the last MSM (see zkp_ntt_profile_enable). */
 void zkp_msm_profile_enable(int on);
 int zkp_msm_profile_read(float *ms, const char **names, int max);

@@ -998,3 +998,54 @@ extern "C" cudaError_t msm_precompute(unsigned long long len, unsigned int *cons
     cudaFree(d);
     return err;
 }
+
+// ------------------------------------------------------------------ allocation-free entry
+// Some callers cannot allocate device memory: a plugin whose host application hands it only
+// input and output buffers and owns every allocator, or a serving loop that must never call
+// cudaMalloc because it synchronises the whole device.  For them zkp_msm_device_noalloc runs
+// the same MSM with its workspace in this fixed array instead of a caller buffer.  The array
+// lives in the library image, so every GPU that loads the library holds it until the process
+// exits.
+static constexpr unsigned long long kNoAllocScratchBytes = 64ull << 20;  // 64 MiB
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+// Host code must not use `g_noalloc_scratch` as a device address (on the host it names a
+// stand-in), so each device's real address is looked up once, with that device current.
+static std::mutex g_noalloc_mu;
+static void *g_noalloc_ptr[64] = {nullptr};
+
+static cudaError_t noalloc_scratch(void **out) {
+    int dev = 0;
+    ZK_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> g(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return cudaSuccess;
+}
+
+extern "C" unsigned long long zkp_msm_noalloc_capacity(void) { return kNoAllocScratchBytes; }
+
+extern "C" cudaError_t zkp_msm_device_noalloc(const unsigned int *points_d, unsigned int n_tables,
+                                              const unsigned int *scalars_d, unsigned long long n,
+                                              unsigned int window, unsigned int *result_d, cudaStream_t stream) {
+    ZK_CHECK_ARG(result_d != nullptr);
+    if (n == 0) return cudaMemsetAsync(result_d, 0, 64, stream);
+    ZK_CHECK_ARG(points_d != nullptr && scalars_d != nullptr);
+    u32 c, nt;
+    msm::resolve(n, window, n_tables, &c, &nt);
+    ZK_CHECK_ARG(c >= 2 && c <= 24 && nt >= 1);
+    ZK_CHECK_ARG(n * nt < (1ull << 31));
+    const msm::Batch b = msm::single(points_d, nt, scalars_d, n, c, result_d);
+    const msm::Layout l = msm::make_layout(b);
+    // larger problems do not fit the fixed scratch: refuse instead of overrunning it
+    if (l.total > kNoAllocScratchBytes) return cudaErrorInvalidValue;
+    void *scratch = nullptr;
+    ZK_TRY(noalloc_scratch(&scratch));
+    return msm::run_batch(b, l, reinterpret_cast<char *>(scratch), stream);
+}

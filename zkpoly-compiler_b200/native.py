@@ -60,6 +60,9 @@ SIGNATURES = {
         "zkp_msm_precompute_device": (cudaError_t, [c_void_p, ctypes.c_ulonglong, ctypes.c_uint, ctypes.c_uint,
                                                     c_void_p]),
         "zkp_msm_batch_workspace_size": (ctypes.c_ulonglong, [c_void_p, ctypes.c_uint]),
+        "zkp_msm_device_noalloc": (cudaError_t, [c_void_p, ctypes.c_uint, c_void_p, ctypes.c_ulonglong,
+                                                 ctypes.c_uint, c_void_p, c_void_p]),
+        "zkp_msm_noalloc_capacity": (ctypes.c_ulonglong, []),
         "zkp_msm_batch": (cudaError_t, [c_void_p, ctypes.c_uint, c_void_p, ctypes.c_ulonglong, c_void_p]),
         "zkp_msm_profile_enable": (None, [ctypes.c_int]),
         "zkp_msm_profile_read": (ctypes.c_int, [ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_char_p),
