@@ -417,11 +417,21 @@ def emit(args, zk, rank, world, n_msm, n_ntt, ntt_ms, msm_ms, step_ms, pass_ms, 
     pass_avg = statistics.median(pass_ms)
     ntt_bytes_per_pass = 64 * n_ntt  # one read + one write of every element per pass
     acc_ms = stage_ms.get("accumulate", float("nan"))
-    msm_mults = 160 * n_msm + 2 * (1 << 15) * 16 * 14  # accounted Fq products (c = 16 accounting)
+    # accounted Fq products: 8 products + 2 squarings per mixed addition, one addition per
+    # (scalar, window) digit; bucket reduction: 2 full additions (12 + 2) per bucket
+    c_msm = bases.window
+    w_msm = (254 + c_msm - 1) // c_msm
+    wp_msm = (w_msm + bases.n_tables - 1) // bases.n_tables
+    acc_mults = 10 * n_msm * w_msm
+    msm_mults = acc_mults + 28 * wp_msm * (1 << (c_msm - 1))
     imad_per_mult = 264
     msm_total_ms = sum(stage_ms.values())
+    digits = zk.ntt.plan_digits(NTT_LOG)
+    # Fr products of the whole transform: D - 1 twiddled stages of n/2 butterflies per pass,
+    # plus the four-step twist (n products) on every pass but the last
+    ntt_mults = sum((n_ntt // 2) * (d - 1) for d in digits) + n_ntt * (len(digits) - 1)
     launches_per_ntt = zk.ntt.num_passes(NTT_LOG)
-    launches_per_msm = 10
+    launches_per_msm = 14
     line = {
         "metric": METRIC, "value": world * n_msm / (msm_ms / 1e3), "unit": "points/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
@@ -438,7 +448,8 @@ def emit(args, zk, rank, world, n_msm, n_ntt, ntt_ms, msm_ms, step_ms, pass_ms, 
         "ntt": {"metric": f"NTT elems/s (2^{NTT_LOG})", "value": world * n_ntt / (ntt_ms / 1e3), "unit": "elems/s",
                 "ms": ntt_ms, "pass_ms": pass_avg, "bitrev_ms": statistics.median(bitrev_ms) if bitrev_ms else None,
                 "hbm_frac_whole_ntt": (64 * n_ntt / (ntt_ms / 1e3) / 1e9) / hbm_peak},
-        "roofline": {"kernel": "ntt_pass_kernel (2^12-point sub-transform pass of the 2^24 NTT)", "bound": "hbm",
+        "roofline": {"kernel": f"ntt_pass_kernel (2^{max(digits)}-point sub-transform passes {digits} of the "
+                               f"2^{NTT_LOG} NTT)", "bound": "hbm",
                      "achieved": ntt_bytes_per_pass / (pass_avg / 1e3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
                      "frac": ntt_bytes_per_pass / (pass_avg / 1e3) / 1e9 / hbm_peak, "peak_source": peak_kind,
                      "traffic": None,
@@ -446,11 +457,13 @@ def emit(args, zk, rank, world, n_msm, n_ntt, ntt_ms, msm_ms, step_ms, pass_ms, 
         "int_roofline": {
             "imad_peak_per_s": imad_per_s, "imad_per_mont_mul": imad_per_mult,
             "mont_mul_peak_per_s": imad_per_s / imad_per_mult,
-            "msm_accumulate": {"kernel": "accumulate_kernel", "ms": acc_ms,
-                               "fq_mults_per_s": msm_mults / (msm_total_ms / 1e3),
-                               "frac_whole_msm": (msm_mults / (msm_total_ms / 1e3)) / (imad_per_s / imad_per_mult)},
-            "ntt_pass": {"fr_mults_per_pass": (n_ntt // 2) * 12,
-                         "frac": ((n_ntt // 2) * 12 / (pass_avg / 1e3)) / (imad_per_s / imad_per_mult)},
+            "msm_accumulate": {"kernel": "accumulate_kernel", "ms": acc_ms, "fq_mults": acc_mults,
+                               "fq_mults_per_s": acc_mults / (acc_ms / 1e3),
+                               "frac": (acc_mults / (acc_ms / 1e3)) / (imad_per_s / imad_per_mult)},
+            "msm_whole": {"fq_mults": msm_mults, "ms": msm_total_ms,
+                          "frac": (msm_mults / (msm_total_ms / 1e3)) / (imad_per_s / imad_per_mult)},
+            "ntt_passes": {"digits": digits, "fr_mults": ntt_mults, "ms": pass_avg * len(digits),
+                           "frac": (ntt_mults / (pass_avg * len(digits) / 1e3)) / (imad_per_s / imad_per_mult)},
         },
         "e2e": {"value": world * n_msm / e2e_msm_s if e2e_msm_s == e2e_msm_s else None, "unit": "points/s",
                 "h2d_bytes_per_step": n_msm * (64 + 32) + n_ntt * 32, "d2h_bytes_per_step": 64 + n_ntt * 32,

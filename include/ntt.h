@@ -67,6 +67,11 @@ cudaError_t zkp_ntt_roots_device(unsigned int *out_d, unsigned long long count, 
  * a smaller cap means more passes of smaller CTAs.  Plans made after the call use it. */
 cudaError_t zkp_ntt_set_max_digit(unsigned int log_len, unsigned int max_digit);
 
+/* The digit widths, top digit first, of the sub-transform passes the current plan for
+ * 2^log_len uses (at most max written); returns the number of passes (0 if log_len is 0 or
+ * above 28). */
+unsigned int zkp_ntt_plan_digits(unsigned int log_len, unsigned int *digits, unsigned int max);
+
 /* Number of sub-transform passes + permutation passes the plan for 2^log_len uses. */
 unsigned int zkp_ntt_num_passes(unsigned int log_len);
 

@@ -186,3 +186,30 @@ def test_ntt_batch_uneven_sizes(zk, orc):
     torch.cuda.synchronize()
     for x, y in zip(xs, ys):
         assert np.array_equal(x.numpy_u64(), y.numpy_u64())
+
+
+@pytest.mark.parametrize("log_n", [9, 13, 17, 20])
+def test_digit_caps_give_the_same_transform(zk, orc, log_n):
+    """Every plan the tuner can pick (digit cap 4..12: more passes of smaller pencils) computes
+    the same transform, forward, coset and inverse."""
+    lib = zk.native.load("libntt.so")
+    n = 1 << log_n
+    a = orc.gen_fr(90 + log_n, n)
+    expect = orc.best_fft(a, orc.root_of_unity(log_n), log_n)
+    g = orc.to_mont(orc.int_to_limbs(7))
+    expect_coset = orc.coset_ntt(a, log_n, log_n, g)
+    try:
+        for d in (4, 5, 7, 8, 10, 11, 12):
+            assert lib.zkp_ntt_set_max_digit(log_n, d) == 0
+            x = to_dev(zk, a)
+            zk.ntt.ssip_ntt(x, zk.ntt.twiddle_table(log_n))
+            assert np.array_equal(x.numpy_u64(), expect), d
+            y = to_dev(zk, a)
+            zk.ntt.ntt_ex(y, zk.ntt.twiddle_table(log_n), zk.ntt.scalar_const(7))
+            assert np.array_equal(y.numpy_u64(), expect_coset), d
+            zk.ntt.intt(x)
+            assert np.array_equal(x.numpy_u64(), a), d
+    finally:
+        assert lib.zkp_ntt_set_max_digit(log_n, 0) == 0
+        zk.tuner.apply_ntt_plans()  # back to the tuned plan, if one is cached
+    assert lib.zkp_ntt_set_max_digit(log_n, 3) != 0 and lib.zkp_ntt_set_max_digit(log_n, 13) != 0

@@ -354,7 +354,10 @@ ZK_DI G1A fetch_point(const u32 *points, u32 code) {
 // the previous chunk, ends here), 2 = head run that also continues into the next chunk,
 // 3 = tail run (starts here, continues into the next).  Buckets of different tasks never
 // share a key, so runs never span two tasks.
-__global__ void __launch_bounds__(256, 2) accumulate_kernel(const Batch b, const u32 *sorted_bucket,
+#ifndef ZK_ACC_MIN_BLOCKS
+#define ZK_ACC_MIN_BLOCKS 2  // resident CTAs of 256 threads per SM the register budget targets
+#endif
+__global__ void __launch_bounds__(256, ZK_ACC_MIN_BLOCKS) accumulate_kernel(const Batch b, const u32 *sorted_bucket,
                                                            const u32 *sorted_point, const u32 *live,
                                                            u32 *bucket_sums, u32 *part_pts, u32 *part_bucket,
                                                            u32 *part_flag) {

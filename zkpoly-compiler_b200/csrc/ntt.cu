@@ -315,8 +315,8 @@ __global__ void __launch_bounds__(256) powers_kernel(u32 *out, const u32 *unit, 
 // ------------------------------------------------------------------ host plan
 struct Plan {
     u32 np;
-    u32 D[4];
-    u32 lo[4];
+    u32 D[8];  // up to ceil(28 / 4) passes
+    u32 lo[8];
 };
 
 // Per-size cap on the digit width (the sub-transform size 2^D of a pass), set by the tuner
@@ -630,6 +630,13 @@ extern "C" cudaError_t zkp_ntt_set_max_digit(unsigned int log_len, unsigned int 
         ntt::g_max_digit[log_len].store(max_digit);
     }
     return cudaSuccess;
+}
+
+extern "C" unsigned int zkp_ntt_plan_digits(unsigned int log_len, unsigned int *digits, unsigned int max) {
+    if (log_len == 0 || log_len > 28) return 0;
+    const ntt::Plan p = ntt::make_plan(log_len);
+    for (u32 i = 0; i < p.np && i < max && digits; i++) digits[i] = p.D[i];
+    return p.np;
 }
 
 extern "C" unsigned int zkp_ntt_num_passes(unsigned int log_len) {

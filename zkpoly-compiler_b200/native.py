@@ -39,6 +39,7 @@ SIGNATURES = {
         "zkp_coset_lde": (cudaError_t, [PolyPtr, PolyPtr, c_void_p, ctypes.c_uint, ctypes.c_uint, c_void_p,
                                         c_void_p]),
         "zkp_ntt_num_passes": (ctypes.c_uint, [ctypes.c_uint]),
+        "zkp_ntt_plan_digits": (ctypes.c_uint, [ctypes.c_uint, c_void_p, ctypes.c_uint]),
         "zkp_ntt_set_max_digit": (cudaError_t, [ctypes.c_uint, ctypes.c_uint]),
         "zkp_ntt_batch_plan_create": (cudaError_t, [c_void_p, ctypes.c_uint, ctypes.POINTER(c_void_p)]),
         "zkp_ntt_batch_run": (cudaError_t, [c_void_p, c_void_p]),

@@ -111,8 +111,15 @@ def coset_lde(out: ScalarArray, inp: ScalarArray, twiddle: ScalarArray, shift: t
                                _log2_exact(out.len), _ptr(shift), stream_handle(stream)), "zkp_coset_lde")
 
 
+def plan_digits(log_len: int) -> list[int]:
+    """Digit widths (top first) of the passes the current plan for 2^log_len uses."""
+    buf = (ctypes.c_uint * 8)()
+    k = _lib().zkp_ntt_plan_digits(log_len, buf, 8)
+    return [int(buf[i]) for i in range(k)]
+
+
 def num_passes(log_len: int) -> int:
-    return int(load(LIB).zkp_ntt_num_passes(log_len))
+    return int(_lib().zkp_ntt_num_passes(log_len))
 
 
 # ------------------------------------------------------------------ cached constants
