@@ -259,6 +259,10 @@ def run_gpu(args):
     torch.cuda.synchronize()
     imad_per_s = 5 * sms * 8 * 256 * iters * 16 / (e0.elapsed_time(e1) / 1e3)
 
+    # ---- fused quotient kernel on the 2^24 extended coset (north_star's fused-kernel roofline)
+    fused = measure_fused(zk, gen, dev, stream, hbm_peak=peaks()[0],
+                          mont_peak=imad_per_s / 264) if not args.no_fused else None
+
     # ---- batched form (mixed NTT/MSM workload) and served form (Poisson arrivals)
     batched = measure_batched(zk, args) if (not args.no_batched and rank == 0) else None
     served = measure_served(zk, bases, args) if (not args.no_served and rank == 0) else None
@@ -274,7 +278,41 @@ def run_gpu(args):
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_reference(args.ref_msm_log, args.ref_ntt_log)
     emit(args, zk, rank, world, n_msm, n_ntt, ntt_ms, msm_ms, step_ms, pass_ms, bitrev_ms, stage_ms, imad_per_s,
-         e2e_msm_s, e2e_ntt_s, cpu, clocks, bases, batched, served)
+         e2e_msm_s, e2e_ntt_s, cpu, clocks, bases, batched, served, fused)
+
+
+def measure_fused(zk, gen, dev, stream, hbm_peak, mont_peak, log_n=NTT_LOG, ext=3, reps=10):
+    """q = (a*b - c - z*z(wX)) * Z_H^-1 over 2^log_n coset points (distinct a, b, c, z): 4 reads +
+    1 write of 32 B per element (z(wX) is the same z one row on, served from cache) and 3 products
+    (a*b, z*z(wX), and the product with the periodic 1/Z_H)."""
+    import torch
+    n = 1 << log_n
+    with torch.cuda.stream(stream):
+        a, b, c, z = (zk.ScalarArray(gen.fr(600 + i, n, dev)) for i in range(4))
+        q = zk.ScalarArray.alloc(n, dev)
+    zh = zk.pipeline.zh_inv_device(log_n - ext, ext, dev)
+    kern = zk.fused.quotient_kernel()
+    args_ = ([q], [a, b, c, z, zk.pipeline.rotated(z, ext), zh])
+    torch.cuda.synchronize()
+    for _ in range(3):
+        kern(*args_, stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        kern(*args_, stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    gbs = 160 * n / (ms / 1e3) / 1e9
+    mults = 3 * n
+    out = {"kernel": "zkp_quotient_z8_kernel (generated fused kernel)", "n": n, "ms": ms,
+           "achieved_gbs": gbs, "hbm_peak_gbs": hbm_peak, "hbm_frac": gbs / hbm_peak,
+           "fr_mults_per_s": mults / (ms / 1e3), "mont_frac": mults / (ms / 1e3) / mont_peak,
+           "bytes_per_elem": 160, "fr_mults_per_elem": 3}
+    del a, b, c, z, q
+    torch.cuda.empty_cache()
+    return out
 
 
 def measure_batched(zk, args, reps=3):
@@ -407,7 +445,7 @@ def run_e2e(zk, native, lib_msm, scalars, points, ntt_in, tw, stream, dev, local
 
 
 def emit(args, zk, rank, world, n_msm, n_ntt, ntt_ms, msm_ms, step_ms, pass_ms, bitrev_ms, stage_ms, imad_per_s,
-         e2e_msm_s, e2e_ntt_s, cpu, clocks, bases, batched=None, served=None):
+         e2e_msm_s, e2e_ntt_s, cpu, clocks, bases, batched=None, served=None, fused=None):
     import torch
     if rank != 0:
         if world > 1:
@@ -472,6 +510,8 @@ def emit(args, zk, rank, world, n_msm, n_ntt, ntt_ms, msm_ms, step_ms, pass_ms, 
         "gpu_launches": args.steps * (launches_per_ntt + launches_per_msm),
         "clocks": clocks.summary(),
     }
+    if fused:
+        line["fused"] = fused
     if batched:
         line["batched"] = batched
     if served:
@@ -494,6 +534,7 @@ def main():
     ap.add_argument("--window", type=int, default=0)
     ap.add_argument("--tables", type=int, default=0, help="precomputed point tables (0 = tuned / full)")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-fused", action="store_true")
     ap.add_argument("--no-served", action="store_true")
     ap.add_argument("--served-requests", type=int, default=120)
     ap.add_argument("--ref-msm-log", type=int, default=22)

@@ -288,6 +288,54 @@ __global__ void __launch_bounds__(256) bitrev_kernel(View v, u32 L, u64 n) {
     }
 }
 
+// Tiled in-place bit reversal for L >= 2 * BR_T.  An index is (a, m, b): a the top BR_T bits,
+// b the low BR_T bits, m the L - 2 BR_T middle bits, and rev(a, m, b) = (rev b, rev m, rev a).
+// CTA m (m <= rev m) owns tiles m and rev m (every (a, b) of that middle value), reads both
+// into shared memory row by row (a row is 2^BR_T consecutive elements) and writes element (a, b)
+// of one tile to (rev b, rev a) of the other, again row by row, so every global access is a
+// run of 1 KB.  Shared memory holds 8 word planes per tile; element (a, b) sits at
+// a * 32 + (b ^ a), which keeps both the row writes and the column reads on 32 banks.
+constexpr u32 BR_T = 5;
+constexpr u32 BR_TILE = 1u << (2 * BR_T);  // elements per tile
+
+__global__ void __launch_bounds__(256) bitrev_tiled_kernel(View v, u32 L) {
+    extern __shared__ u32 br_sm[];  // 2 tiles x 8 planes x BR_TILE words
+    const u32 M = L - 2 * BR_T;
+    const u32 m = blockIdx.x;
+    const u32 mr = M ? (__brev(m) >> (32 - M)) : 0u;
+    if (mr < m) return;  // the pair is handled by CTA mr
+    const u32 ntile = mr == m ? 1 : 2;
+    const u32 lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    const u32 mid[2] = {m, mr};
+    for (u32 t = 0; t < ntile; t++) {
+        u32 *tile = br_sm + t * 8 * BR_TILE;
+        for (u32 a = warp; a < 32; a += nwarp) {
+            const u64 i = ((u64)a << (L - BR_T)) | ((u64)mid[t] << BR_T) | lane;
+            Fr x = Fr::load(v.at(i));
+            const u32 pos = a * 32 + (lane ^ a);
+#pragma unroll
+            for (int w = 0; w < 8; w++) tile[w * BR_TILE + pos] = x.v[w];
+        }
+    }
+    __syncthreads();
+    for (u32 t = 0; t < ntile; t++) {
+        // destination tile mid[t] receives the other tile (itself when the pair is one tile)
+        const u32 *src = br_sm + (ntile == 2 ? 1 - t : 0) * 8 * BR_TILE;
+        for (u32 ao = warp; ao < 32; ao += nwarp) {
+            // element (ao, lane) of the destination = element (rev lane, rev ao) of the source
+            const u32 a = __brev(lane) >> 27, b = __brev(ao) >> 27;
+            const u32 pos = a * 32 + (b ^ a);
+            Fr x;
+#pragma unroll
+            for (int w = 0; w < 8; w++) x.v[w] = src[w * BR_TILE + pos];
+            const u64 i = ((u64)ao << (L - BR_T)) | ((u64)mid[t] << BR_T) | lane;
+            x.store(v.at(i));
+        }
+    }
+}
+
+constexpr size_t BR_SMEM = 2 * 8 * BR_TILE * sizeof(u32);  // 64 KiB
+
 __global__ void __launch_bounds__(256) distribute_powers_kernel(View v, const u32 *powers, u64 pn, u64 n) {
     const u64 stride = (u64)gridDim.x * blockDim.x;
     for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
@@ -351,6 +399,7 @@ inline Plan make_plan(u32 L) {
 
 std::atomic<uint64_t> g_attr_done{0};
 std::atomic<uint64_t> g_batch_attr_done{0};
+std::atomic<uint64_t> g_br_attr_done{0};
 
 inline size_t pass_smem(u32 D) {
     const size_t S = 1u << D, H = S > 1 ? S / 2 : 1;
@@ -413,9 +462,14 @@ cudaError_t run(const View &v, const View *src, u64 src_len, u32 L, const u32 *t
     }
     if (plan.np > 1) {
         const u64 n = 1ull << L;
-        const u64 blocks = (n / 2 + 255) / 256;
-        const u32 grid = (u32)(blocks < (u64)num_sms() * 16 ? blocks : (u64)num_sms() * 16);
-        bitrev_kernel<<<grid, 256, 0, stream>>>(v, L, n);
+        if (L >= 2 * BR_T) {
+            ZK_TRY(ensure_smem_attr(bitrev_tiled_kernel, (int)BR_SMEM, g_br_attr_done));
+            bitrev_tiled_kernel<<<1u << (L - 2 * BR_T), 256, BR_SMEM, stream>>>(v, L);
+        } else {
+            const u64 blocks = (n / 2 + 255) / 256;
+            const u32 grid = (u32)(blocks < (u64)num_sms() * 16 ? blocks : (u64)num_sms() * 16);
+            bitrev_kernel<<<grid, 256, 0, stream>>>(v, L, n);
+        }
         ZK_TRY(cudaGetLastError());
         profiler().mark("bitrev", stream);
     }
