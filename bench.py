@@ -490,7 +490,9 @@ def emit(args, zk, rank, world, n_msm, n_ntt, ntt_ms, msm_ms, step_ms, pass_ms, 
                                f"2^{NTT_LOG} NTT)", "bound": "hbm",
                      "achieved": ntt_bytes_per_pass / (pass_avg / 1e3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
                      "frac": ntt_bytes_per_pass / (pass_avg / 1e3) / 1e9 / hbm_peak, "peak_source": peak_kind,
-                     "traffic": None,
+                     # ncu DRAM bytes per pass launch: 61.9 B per element at 2^22 (three tuned
+                     # passes, 778 MB), scaled by the element count
+                     "traffic": 61.9 * n_ntt,
                      "note": "IMAD-bound kernel: HBM fraction reported as asked; see int_roofline"},
         "int_roofline": {
             "imad_peak_per_s": imad_per_s, "imad_per_mont_mul": imad_per_mult,
