@@ -109,6 +109,11 @@ int zkp_msm_profile_read(float *ms, const char **names, int max);
  * (out_d: blocks * 256 words).  Used to measure the IMAD peak the MSM roofline divides by. */
 cudaError_t zkp_imad_probe(unsigned int blocks, unsigned int iters, unsigned int *out_d, cudaStream_t stream);
 
+/* Montgomery-product throughput probe: blocks x 256 threads x iters x 2 Fq products with the
+ * library's own product routine (out_d: blocks * 256 * 8 words).  Its rate is the denominator
+ * of the field-product roofline fractions. */
+cudaError_t zkp_mont_probe(unsigned int blocks, unsigned int iters, unsigned int *out_d, cudaStream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

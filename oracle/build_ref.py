@@ -1,7 +1,18 @@
-"""Builds oracle/_ref/libref.so (test infrastructure): oracle/ref_driver.cu compiled against the
-reference's own headers where they lie under the reference checkout (host code only, nvcc as
-the C++ compiler; the reference's build system is not used).  Skipped when the checkout is
-absent; the built library travels with the repository snapshot.
+"""Builds the reference's own code into oracle/_ref/ (test infrastructure only), from the sources
+where they lie in the reference checkout, with nvcc for sm_100a (the reference's build system,
+xmake / Makefile.msm, is not used):
+
+  libref.so                oracle/ref_driver.cu against the reference's host arithmetic headers
+  libref_ntt.so            core/src/ntt/src/ntt.cu (ssip_ntt, ssip_precompute, recompute_ntt,
+                           gen_pq_omegas, distribute_powers) with NTT_FIELD = bn254_fr::Element,
+                           the definition the reference's build uses for BN254
+  libref_msm_<s>_<t>.so    core/src/msm/src/msm.cu with MSM_WINDOW_SIZE = s and
+                           MSM_TARGET_WINDOWS = t (the per-configuration library the reference
+                           builds, Makefile.msm), MSM_BITS 254, curve bn254, debug off
+
+Skipped when the checkout is absent; the built libraries travel with the repository snapshot.
+The GPU libraries serve the parity tests that run the reference's kernels next to this
+repository's on the same inputs.
 
 Usage: python oracle/build_ref.py [reference_root]
 """
@@ -11,25 +22,56 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
-OUT = os.path.join(HERE, "_ref", "libref.so")
+OUT_DIR = os.path.join(HERE, "_ref")
+NVCC = "/usr/local/cuda/bin/nvcc"
+BASE = [NVCC, "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared", "-gencode", "arch=compute_100a,code=sm_100a",
+        "-diag-suppress", "550,177"]
+# (window, target windows): 16/16 is the default library name the reference's runtime loads
+# (one point table); 17/8 is its cost model's choice for 2^22 points (two tables)
+MSM_CONFIGS = [(16, 16), (17, 8)]
+
+
+def jobs():
+    out = []
+    driver = os.path.join(HERE, "ref_driver.cu")
+    out.append((os.path.join(OUT_DIR, "libref.so"), [driver],
+                BASE[:1] + ["-O2"] + BASE[2:] + [
+                    "-I" + os.path.join(REF, "core/src/common/curve/src"),
+                    "-I" + os.path.join(REF, "core/src/ntt/src"),
+                    "-DNTT_FIELD=bn254_fr::Element", driver]))
+    ntt_src = os.path.join(REF, "core/src/ntt/src/ntt.cu")
+    out.append((os.path.join(OUT_DIR, "libref_ntt.so"), [ntt_src],
+                BASE + ["-DNTT_FIELD=bn254_fr::Element", ntt_src]))
+    msm_src = os.path.join(REF, "core/src/msm/src/msm.cu")
+    for s, t in MSM_CONFIGS:
+        out.append((os.path.join(OUT_DIR, f"libref_msm_{s}_{t}.so"), [msm_src],
+                    BASE + ["-I" + os.path.join(REF, "core/src/msm"), "-DMSM_BITS=254", "-DMSM_CURVE=bn254",
+                            f"-DMSM_WINDOW_SIZE={s}", f"-DMSM_TARGET_WINDOWS={t}", "-DMSM_DEBUG=false",
+                            msm_src]))
+    return out
 
 
 def main():
     if not os.path.isdir(REF):
         print("reference checkout absent; oracle/_ref not built")
         return
-    os.makedirs(os.path.dirname(OUT), exist_ok=True)
-    src = os.path.join(HERE, "ref_driver.cu")
-    if os.path.exists(OUT) and os.path.getmtime(OUT) > os.path.getmtime(src):
-        return
-    cmd = ["/usr/local/cuda/bin/nvcc", "-O2", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
-           "-gencode", "arch=compute_100a,code=sm_100a",
-           "-I" + os.path.join(REF, "core/src/common/curve/src"),
-           "-I" + os.path.join(REF, "core/src/ntt/src"),
-           "-DNTT_FIELD=bn254_fr::Element",
-           "-o", OUT, src]
-    subprocess.run(cmd, check=True)
-    print(OUT)
+    os.makedirs(OUT_DIR, exist_ok=True)
+    running = []
+    for target, srcs, cmd in jobs():
+        if os.path.exists(target) and all(os.path.getmtime(target) > os.path.getmtime(s) for s in srcs):
+            continue
+        running.append((target, subprocess.Popen(cmd + ["-o", target + ".tmp"], stdout=subprocess.PIPE,
+                                                 stderr=subprocess.STDOUT, text=True)))
+    failed = []
+    for target, proc in running:
+        log, _ = proc.communicate()
+        if proc.returncode != 0:
+            failed.append(f"{target}:\n{log}")
+        else:
+            os.replace(target + ".tmp", target)
+            print(target)
+    if failed:
+        raise RuntimeError("reference build failed:\n" + "\n".join(failed))
 
 
 if __name__ == "__main__":

@@ -1,0 +1,160 @@
+"""The reference's own CUDA kernels, built from its sources into oracle/_ref (oracle/build_ref.py),
+run next to this repository's kernels on the same inputs: NTT (ssip_ntt) and MSM (msm, two of the
+reference's library configurations) must agree bit for bit.  Skipped when oracle/_ref was not
+built (no reference checkout where the libraries were built).
+
+With ZKP_REF_TIMING=1 the tests also time both sides (CUDA events for the NTT, host clock for
+the synchronous host-buffer MSM ABI) and print one JSON line per comparison."""
+import ctypes
+import json
+import os
+import time
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+REF_DIR = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref")
+TIMING = os.environ.get("ZKP_REF_TIMING") == "1"
+
+
+def _ref_lib(name):
+    path = os.path.join(REF_DIR, name)
+    if not os.path.exists(path):
+        pytest.skip(f"{name} not built (reference checkout absent at build time)")
+    return ctypes.CDLL(path)
+
+
+def _ref_ntt(zk):
+    lib = _ref_lib("libref_ntt.so")
+    lib.ssip_ntt.restype = ctypes.c_int
+    lib.ssip_ntt.argtypes = [zk.native.PolyPtr, ctypes.c_void_p, ctypes.c_uint, ctypes.c_void_p, ctypes.c_uint,
+                             ctypes.c_uint]
+    return lib
+
+
+def _ref_msm(name):
+    lib = _ref_lib(name)
+    lib.msm.restype = ctypes.c_int
+    lib.msm.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_ulonglong, ctypes.c_uint, ctypes.c_uint,
+                        ctypes.c_uint, ctypes.c_uint, ctypes.c_uint, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint,
+                        ctypes.c_void_p, ctypes.c_void_p]
+    lib.msm_precompute.restype = ctypes.c_int
+    lib.msm_precompute.argtypes = [ctypes.c_ulonglong, ctypes.c_void_p, ctypes.c_uint]
+    return lib
+
+
+def _call_msm(lib, n, tables, scalars, parts, stages):
+    """One call of the reference-ABI msm with host tables and host scalar batches (the runtime's
+    call, core/src/msm.rs:302-369); returns the affine results and the host-clock seconds."""
+    cards = (ctypes.c_uint * 1)(0)
+    sizes = (ctypes.c_ulong * 1)()
+    assert lib.msm(None, sizes, n, 1, parts, stages, stages, 1, cards, None, 0, None, None) == 0
+    buf = torch.empty(int(sizes[0]), dtype=torch.uint8, device="cuda")
+    bufs = (ctypes.c_void_p * 1)(buf.data_ptr())
+    h_points = (ctypes.c_void_p * len(tables))(*[t.ctypes.data for t in tables])
+    h_scal = (ctypes.c_void_p * len(scalars))(*[s.ctypes.data for s in scalars])
+    results = [np.zeros(16, dtype=np.uint32) for _ in scalars]
+    h_res = (ctypes.c_void_p * len(results))(*[r.ctypes.data for r in results])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    rc = lib.msm(bufs, None, n, 1, parts, stages, stages, 1, cards, h_points, len(scalars), h_scal, h_res)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    assert rc == 0
+    return results, dt
+
+
+def _pinned_u32(t: torch.Tensor) -> np.ndarray:
+    return t.cpu().pin_memory().numpy().view(np.uint32)
+
+
+@pytest.mark.parametrize("log_n", [4, 10, 13, 16, 20, 24])
+def test_reference_ssip_ntt_matches(zk, log_n):
+    ref = _ref_ntt(zk)
+    n = 1 << log_n
+    data = zk.gen.fr(300 + log_n, n)
+    tw = zk.ntt.twiddle_table(log_n)
+    x_ref, x = zk.ScalarArray(data.clone()), zk.ScalarArray(data.clone())
+    stream = torch.cuda.current_stream().cuda_stream
+    assert ref.ssip_ntt(x_ref.poly_ptr(), tw.values.data_ptr(), log_n, stream, 8, 8) == 0
+    zk.ntt.ssip_ntt(x, tw)
+    torch.cuda.synchronize()
+    assert torch.equal(x_ref.values, x.values)
+    if TIMING and log_n >= 20:
+        def t(fn, reps=5):
+            fn()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(reps):
+                fn()
+            e1.record()
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1) / reps
+        ms_ref = t(lambda: ref.ssip_ntt(x_ref.poly_ptr(), tw.values.data_ptr(), log_n, stream, 8, 8))
+        ms = t(lambda: zk.ntt.ssip_ntt(x, tw))
+        print(json.dumps({"compare": "ssip_ntt", "log_n": log_n, "reference_ms": ms_ref, "this_ms": ms,
+                          "speedup": ms_ref / ms}))
+
+
+@pytest.mark.parametrize("log_n", [10, 16])
+def test_reference_msm_one_table_matches(zk, log_n):
+    """The runtime's default library (window 16, 16 target windows: one table)."""
+    ref = _ref_msm("libref_msm_16_16.so")
+    n = 1 << log_n
+    pts = _pinned_u32(zk.gen.points(2, n))
+    scal = [_pinned_u32(zk.gen.fr(400 + i, n)) for i in range(2)]
+    got, _ = _call_msm(ref, n, [pts], scal, parts=1, stages=1)
+    ours = zk.msm.msm_host_batches(scal, [pts])
+    for a, b in zip(got, ours):
+        assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("log_n", [16, 20, 22])
+def test_reference_msm_precomputed_matches(zk, log_n):
+    """The reference cost model's configuration for 2^22 points (window 17, 8 target windows:
+    two point tables built by the reference's msm_precompute, 16 parts, two stages)."""
+    if log_n == 22 and not TIMING:
+        pytest.skip("2^22 runs with ZKP_REF_TIMING=1")
+    ref = _ref_msm("libref_msm_17_8.so")
+    n = 1 << log_n
+    pts_dev = zk.gen.points(2, n)
+    tables = [_pinned_u32(pts_dev), np.zeros((n, 16), dtype=np.uint32)]
+    h_tab = (ctypes.c_void_p * 2)(*[t.ctypes.data for t in tables])
+    assert ref.msm_precompute(n, h_tab, 1) == 0
+    scal_dev = zk.gen.fr(500, n)
+    scal = [_pinned_u32(scal_dev)]
+    parts = 16 if n >= (1 << 16) else 1
+    got, dt_ref = _call_msm(ref, n, tables, scal, parts=parts, stages=2 if parts > 1 else 1)
+    ours = zk.msm.msm_host_batches(scal, [tables[0]])
+    assert np.array_equal(got[0], ours[0])
+    if TIMING:
+        # best of 3 for both sides; this repository's side twice: the same host-buffer ABI (one
+        # table) and the device-resident form with the tuned precomputed tables
+        dt_ref = min(dt_ref, *[_call_msm(ref, n, tables, scal, parts, 2)[1] for _ in range(2)])
+        dt = []
+        for _ in range(3):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            zk.msm.msm_host_batches(scal, [tables[0]])
+            torch.cuda.synchronize()
+            dt.append(time.perf_counter() - t0)
+        c, nt = zk.tuner.msm_resident_config(n)
+        rb = zk.msm.ResidentBases(pts_dev, window=c, n_tables=nt)
+        ws = rb.workspace()
+        res = torch.zeros(16, dtype=torch.int32, device="cuda")
+        rb.msm(scal_dev, res, ws)
+        torch.cuda.synchronize()
+        assert np.array_equal(res.cpu().numpy().view(np.uint32), got[0])
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(5):
+            rb.msm(scal_dev, res, ws)
+        e1.record()
+        torch.cuda.synchronize()
+        print(json.dumps({"compare": "msm host-buffer ABI", "log_n": log_n, "reference_s17_t8_ms": dt_ref * 1e3,
+                          "this_abi_ms": min(dt) * 1e3, "this_resident_ms": e0.elapsed_time(e1) / 5,
+                          "resident_config": [c, nt]}))

@@ -803,6 +803,36 @@ extern "C" cudaError_t zkp_imad_probe(unsigned int blocks, unsigned int iters, u
     return cudaGetLastError();
 }
 
+// Montgomery-product throughput probe for the field-product roofline: every thread runs two
+// independent chains of `iters` Fq products (x = x * y) from values derived from its index.
+__global__ void __launch_bounds__(256) mont_probe_kernel(u32 iters, u32 *out) {
+    const u32 tid = blockIdx.x * blockDim.x + threadIdx.x;
+    Fq x, y, u, v;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        x.v[k] = (tid + 1) * 0x9e3779b9u + k * 0x85ebca6bu;
+        y.v[k] = (tid + 7) * 0xc2b2ae35u + k * 0x27d4eb2fu;
+        u.v[k] = x.v[k] ^ 0x165667b1u;
+        v.v[k] = y.v[k] ^ 0xd3a2646cu;
+    }
+    x.v[7] &= 0x1fffffffu;  // below the modulus
+    y.v[7] &= 0x1fffffffu;
+    u.v[7] &= 0x1fffffffu;
+    v.v[7] &= 0x1fffffffu;
+    for (u32 i = 0; i < iters; i++) {
+        x = Fq::mul(x, y);
+        u = Fq::mul(u, v);
+    }
+    Fq::add(x, u).store(out + (u64)tid * 8);
+}
+
+// blocks x 256 threads x iters x 2 Fq products; out_d holds blocks * 256 * 8 words
+extern "C" cudaError_t zkp_mont_probe(unsigned int blocks, unsigned int iters, unsigned int *out_d,
+                                      cudaStream_t stream) {
+    mont_probe_kernel<<<blocks, 256, 0, stream>>>(iters, out_d);
+    return cudaGetLastError();
+}
+
 extern "C" unsigned int zkp_msm_default_window(unsigned long long n) { return msm::default_window(n); }
 
 extern "C" unsigned long long zkp_msm_workspace_size(unsigned long long n, unsigned int window, unsigned int n_tables) {

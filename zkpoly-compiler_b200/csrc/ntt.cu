@@ -250,6 +250,93 @@ __global__ void __launch_bounds__(MAX_THREADS, 1) ntt_batch_pass_kernel(const Pa
     }
 }
 
+// ------------------------------------------------------------------ register pass (D <= 6)
+// The same pass as pass_body written as the global radix-2 DIF stages it equals (the four-step
+// twist of pass_body is folded into the stage twiddles): stage s pairs i and i + 2^s and
+// multiplies the difference by w^((i mod 2^s) * 2^(L-1-s)), read from the caller's root
+// table.  A pencil of 2^D elements lives in the registers of g = 2^(D-1) lanes, two elements
+// per lane: lane l starts with local indices l and l + g, so the first stage is a butterfly
+// inside the lane.  Before each later stage (local bit k) the lane bit k and the register bit
+// trade places through one shuffle of one element per lane, bringing the stage's partners
+// into the same lane; after the last stage lane l holds local indices 2l and 2l + 1.  Each
+// lane group works on two pencils that differ only in their top index bits where there are
+// any, so both pencils use the same twiddle and every twiddle load feeds two products.  No
+// shared memory and no block barrier; every element is one 32-byte sector in and out.
+constexpr u32 WARP_MAX_D = 6;
+
+ZK_DI void lane_swap(Fr &a, Fr &b, u32 lane, u32 k) {
+    const bool hi = (lane >> k) & 1u;
+    Fr send = hi ? a : b;
+#pragma unroll
+    for (int w = 0; w < 8; w++) send.v[w] = __shfl_xor_sync(0xffffffffu, send.v[w], 1u << k);
+    if (hi) a = send; else b = send;
+}
+
+__global__ void __launch_bounds__(256) ntt_warp_pass_kernel(PassArgs a) {
+    const u32 D = a.D, lo = a.lo, L = a.L;
+    const u32 g = 1u << (D - 1);  // lanes per pencil pair
+    const u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    const u64 pair = t >> (D - 1);
+    const u32 l = (u32)t & (g - 1);
+    const u32 lane = threadIdx.x & 31;
+    // pencils q and q + half of the 2^(L-D) pencils (q = h * 2^lo + c)
+    const u64 half = 1ull << (L - D - 1);
+    const u64 cmask = (1ull << lo) - 1;
+    u64 base[2], c[2];
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+        const u64 q = pair + (j ? half : 0);
+        c[j] = q & cmask;
+        base[j] = ((q >> lo) << (lo + D)) | c[j];
+    }
+    const bool shared_tw = c[0] == c[1];
+    Fr x0[2], x1[2];
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+        x0[j] = Fr::load(a.v.at(base[j] + ((u64)l << lo)));
+        x1[j] = Fr::load(a.v.at(base[j] + ((u64)(l + g) << lo)));
+    }
+    for (int k = (int)D - 1; k >= 0; k--) {
+        if (k < (int)D - 1) {
+#pragma unroll
+            for (int j = 0; j < 2; j++) lane_swap(x0[j], x1[j], lane, (u32)k);
+        }
+        const u64 low = (u64)(l & ((1u << k) - 1)) << lo;
+        const u32 sh = L - 1 - lo - (u32)k;
+        Fr w;
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+            const u64 e = (low | c[j]) << sh;
+            Fr s = Fr::add(x0[j], x1[j]);
+            Fr d = Fr::sub(x0[j], x1[j]);
+            if (e != 0) {
+                if (j == 0 || !shared_tw) w = Fr::load_nc(a.tw + e * 8);
+                d = Fr::mul(d, w);
+            }
+            x0[j] = s;
+            x1[j] = d;
+        }
+    }
+    const bool canon = (a.flags & F_CANON) != 0;
+    const bool postscale = (a.flags & F_POSTSCALE) != 0;
+    Fr scale;
+    if (postscale) scale = Fr::load_nc(a.scale);
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+        Fr y0 = x0[j], y1 = x1[j];
+        if (postscale) {
+            y0 = Fr::mul(y0, scale);
+            y1 = Fr::mul(y1, scale);
+        }
+        if (canon) {
+            y0 = y0.canonical();
+            y1 = y1.canonical();
+        }
+        y0.store(a.v.at(base[j] + ((u64)(2 * l) << lo)));
+        y1.store(a.v.at(base[j] + ((u64)(2 * l + 1) << lo)));
+    }
+}
+
 // batched in-place bit reversal: element w of the concatenation belongs to task t
 __global__ void __launch_bounds__(256) bitrev_batch_kernel(const View *views, const u32 *logs, const u64 *first,
                                                           u32 ntasks) {
@@ -406,7 +493,21 @@ inline size_t pass_smem(u32 D) {
     return (8 * S + 8 * H + 8 * 128) * sizeof(u32);
 }
 
+// The register pass handles table-mode passes of at most 2^6-point pencils without a source,
+// coset shift or natural-order store (pass_body does those), on at least 2^7 elements so that
+// every warp is full.
+inline bool warp_pass_ok(const PassArgs &a) {
+    return a.D >= 1 && a.D <= WARP_MAX_D && a.L >= 7 &&
+           (a.flags & (F_RECOMPUTE | F_PRESHIFT | F_SRC | F_NATURAL)) == 0;
+}
+
 cudaError_t launch_pass(const PassArgs &a, cudaStream_t stream) {
+    if (warp_pass_ok(a)) {
+        const u64 threads = 1ull << (a.L - 2);  // two elements of two pencils per thread
+        ntt_warp_pass_kernel<<<(u32)(threads / 256 > 0 ? threads / 256 : 1),
+                               (u32)(threads < 256 ? threads : 256), 0, stream>>>(a);
+        return cudaGetLastError();
+    }
     ZK_TRY(ensure_smem_attr(ntt_pass_kernel, (int)pass_smem(MAX_D), g_attr_done));
     const u64 pencils = 1ull << (a.L - a.D);
     const u32 H = (1u << a.D) >> 1;

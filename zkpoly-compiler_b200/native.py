@@ -69,6 +69,7 @@ SIGNATURES = {
         "zkp_msm_profile_read": (ctypes.c_int, [ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_char_p),
                                                 ctypes.c_int]),
         "zkp_imad_probe": (cudaError_t, [ctypes.c_uint, ctypes.c_uint, c_void_p, c_void_p]),
+        "zkp_mont_probe": (cudaError_t, [ctypes.c_uint, ctypes.c_uint, c_void_p, c_void_p]),
     },
     "libzkp_gen.so": {
         "zkp_gen_fr": (cudaError_t, [ctypes.c_ulonglong, ctypes.c_ulonglong, ctypes.c_ulonglong, c_void_p, c_void_p]),
