@@ -258,9 +258,9 @@ __global__ void __launch_bounds__(MAX_THREADS, 1) ntt_batch_pass_kernel(const Pa
 // per lane: lane l starts with local indices l and l + g, so the first stage is a butterfly
 // inside the lane.  Before each later stage (local bit k) the lane bit k and the register bit
 // trade places through one shuffle of one element per lane, bringing the stage's partners
-// into the same lane; after the last stage lane l holds local indices 2l and 2l + 1.  Each
-// lane group works on two pencils that differ only in their top index bits where there are
-// any, so both pencils use the same twiddle and every twiddle load feeds two products.  No
+// into the same lane; after the last stage lane l holds local indices 2l and 2l + 1.  A lane
+// group works on P pencils (1 or 2); with two, they differ only in their top index bits where
+// there are any, so both use the same twiddle and a twiddle load feeds two products.  No
 // shared memory and no block barrier; every element is one 32-byte sector in and out.
 constexpr u32 WARP_MAX_D = 6;
 
@@ -272,40 +272,42 @@ ZK_DI void lane_swap(Fr &a, Fr &b, u32 lane, u32 k) {
     if (hi) a = send; else b = send;
 }
 
+template <u32 D, u32 P>
 __global__ void __launch_bounds__(256) ntt_warp_pass_kernel(PassArgs a) {
-    const u32 D = a.D, lo = a.lo, L = a.L;
-    const u32 g = 1u << (D - 1);  // lanes per pencil pair
+    constexpr u32 g = 1u << (D - 1);  // lanes per pencil group
+    const u32 lo = a.lo, L = a.L;
     const u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x;
-    const u64 pair = t >> (D - 1);
+    const u64 grp = t >> (D - 1);
     const u32 l = (u32)t & (g - 1);
     const u32 lane = threadIdx.x & 31;
-    // pencils q and q + half of the 2^(L-D) pencils (q = h * 2^lo + c)
+    // P pencils per lane group: q = grp + j * 2^(L-D-1) (they differ in the top index bit)
     const u64 half = 1ull << (L - D - 1);
     const u64 cmask = (1ull << lo) - 1;
-    u64 base[2], c[2];
+    u64 base[P], c[P];
 #pragma unroll
-    for (int j = 0; j < 2; j++) {
-        const u64 q = pair + (j ? half : 0);
+    for (u32 j = 0; j < P; j++) {
+        const u64 q = grp + (j ? half : 0);
         c[j] = q & cmask;
         base[j] = ((q >> lo) << (lo + D)) | c[j];
     }
-    const bool shared_tw = c[0] == c[1];
-    Fr x0[2], x1[2];
+    const bool shared_tw = P == 1 || c[0] == c[P - 1];
+    Fr x0[P], x1[P];
 #pragma unroll
-    for (int j = 0; j < 2; j++) {
+    for (u32 j = 0; j < P; j++) {
         x0[j] = Fr::load(a.v.at(base[j] + ((u64)l << lo)));
         x1[j] = Fr::load(a.v.at(base[j] + ((u64)(l + g) << lo)));
     }
+#pragma unroll
     for (int k = (int)D - 1; k >= 0; k--) {
         if (k < (int)D - 1) {
 #pragma unroll
-            for (int j = 0; j < 2; j++) lane_swap(x0[j], x1[j], lane, (u32)k);
+            for (u32 j = 0; j < P; j++) lane_swap(x0[j], x1[j], lane, (u32)k);
         }
         const u64 low = (u64)(l & ((1u << k) - 1)) << lo;
         const u32 sh = L - 1 - lo - (u32)k;
         Fr w;
 #pragma unroll
-        for (int j = 0; j < 2; j++) {
+        for (u32 j = 0; j < P; j++) {
             const u64 e = (low | c[j]) << sh;
             Fr s = Fr::add(x0[j], x1[j]);
             Fr d = Fr::sub(x0[j], x1[j]);
@@ -322,7 +324,7 @@ __global__ void __launch_bounds__(256) ntt_warp_pass_kernel(PassArgs a) {
     Fr scale;
     if (postscale) scale = Fr::load_nc(a.scale);
 #pragma unroll
-    for (int j = 0; j < 2; j++) {
+    for (u32 j = 0; j < P; j++) {
         Fr y0 = x0[j], y1 = x1[j];
         if (postscale) {
             y0 = Fr::mul(y0, scale);
@@ -335,6 +337,26 @@ __global__ void __launch_bounds__(256) ntt_warp_pass_kernel(PassArgs a) {
         y0.store(a.v.at(base[j] + ((u64)(2 * l) << lo)));
         y1.store(a.v.at(base[j] + ((u64)(2 * l + 1) << lo)));
     }
+}
+
+#ifndef ZK_NTT_WARP_PENCILS
+#define ZK_NTT_WARP_PENCILS 1  // pencils per lane group in the register pass (1 or 2)
+#endif
+
+template <u32 P>
+cudaError_t launch_warp_pass(const PassArgs &a, cudaStream_t stream) {
+    const u64 threads = 1ull << (a.L - 1 - (P == 2 ? 1 : 0));  // two elements of P pencils per thread
+    const u32 block = (u32)(threads < 256 ? threads : 256);
+    const u32 grid = (u32)(threads / block);
+    switch (a.D) {
+        case 1: ntt_warp_pass_kernel<1, P><<<grid, block, 0, stream>>>(a); break;
+        case 2: ntt_warp_pass_kernel<2, P><<<grid, block, 0, stream>>>(a); break;
+        case 3: ntt_warp_pass_kernel<3, P><<<grid, block, 0, stream>>>(a); break;
+        case 4: ntt_warp_pass_kernel<4, P><<<grid, block, 0, stream>>>(a); break;
+        case 5: ntt_warp_pass_kernel<5, P><<<grid, block, 0, stream>>>(a); break;
+        default: ntt_warp_pass_kernel<6, P><<<grid, block, 0, stream>>>(a); break;
+    }
+    return cudaGetLastError();
 }
 
 // batched in-place bit reversal: element w of the concatenation belongs to task t
@@ -502,12 +524,7 @@ inline bool warp_pass_ok(const PassArgs &a) {
 }
 
 cudaError_t launch_pass(const PassArgs &a, cudaStream_t stream) {
-    if (warp_pass_ok(a)) {
-        const u64 threads = 1ull << (a.L - 2);  // two elements of two pencils per thread
-        ntt_warp_pass_kernel<<<(u32)(threads / 256 > 0 ? threads / 256 : 1),
-                               (u32)(threads < 256 ? threads : 256), 0, stream>>>(a);
-        return cudaGetLastError();
-    }
+    if (warp_pass_ok(a)) return launch_warp_pass<ZK_NTT_WARP_PENCILS>(a, stream);
     ZK_TRY(ensure_smem_attr(ntt_pass_kernel, (int)pass_smem(MAX_D), g_attr_done));
     const u64 pencils = 1ull << (a.L - a.D);
     const u32 H = (1u << a.D) >> 1;
