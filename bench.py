@@ -388,8 +388,11 @@ def measure_served(zk, bases, args):
                        "3 INTT + coset NTT 4x + fused quotient + 4 MSM (one batch) + 2 evals",
            "hbm_arena_gb": 48}
     burst = [(0.0, k, seed) for _, k, seed in sched]  # every request at once: capacity
+    # resident bases with the tuned (window, tables) per size range
+    sets = zk.serving.resident_sets(bases.tables[: bases.n], 14, 22)
+    out["table_sets"] = [{"max_k": mk, "window": rb.window, "tables": rb.n_tables} for rb, mk in sets]
     for name, inflight in (("served", 8), ("served_1_slot", 1)):
-        srv = zk.serving.Server(bases, hbm_bytes=48 << 30, max_inflight=inflight, ext_log=2, min_k=14, max_k=22)
+        srv = zk.serving.Server(sets, hbm_bytes=48 << 30, max_inflight=inflight, ext_log=2, min_k=14, max_k=22)
         # warm the constants / kernels once
         srv.wait(srv.submit(14, 1))
         _, summary = zk.serving.run_schedule(srv, sched)
@@ -399,6 +402,7 @@ def measure_served(zk, bases, args):
             out["served_capacity"] = cap
         srv.close()
     prover = zk.serving.PerCallProver(bases, ext_log=2, max_k=22)
+    del sets
     prover.warm(range(14, 23))
     prover.run(14, 1)
     torch.cuda.synchronize()

@@ -27,6 +27,19 @@ extern "C" {
 
 typedef struct ZkpServer ZkpServer;
 
+/* One set of resident MSM bases: n_tables tables of `rows` affine points (table j starts at
+ * point j * rows and holds 2^(j*Wp*window) * P).  A request of size k reads the first 2^k rows
+ * of each table. */
+typedef struct ZkpServeTableSet {
+    const unsigned int *tables_d;
+    unsigned long long rows;       /* >= 2^max_k */
+    unsigned int window;           /* 0 = library default per size (one table only) */
+    unsigned int n_tables;
+    unsigned int max_k;            /* the set serves requests of size k <= max_k */
+} ZkpServeTableSet;
+
+#define ZKP_SERVE_MAX_SETS 8
+
 typedef struct ZkpServeConfig {
     unsigned long long hbm_bytes;  /* arena size = admission budget for request buffers */
     unsigned int max_inflight;     /* concurrent requests (streams); 1 = plain per-call path */
@@ -35,6 +48,11 @@ typedef struct ZkpServeConfig {
     unsigned int msm_window;       /* 0 = library default per size (one table only) */
     unsigned int msm_tables;       /* precomputed tables in bases_d (1 = none); table j holds
                                       2^(j*Wp*msm_window) * P for all n_bases points */
+    unsigned int n_sets;           /* 0: one set (bases_d, msm_window, msm_tables) for every
+                                      size; else sets[0..n_sets) by ascending max_k, and a
+                                      request of size k uses the first set with max_k >= k
+                                      (bases_d is then ignored) */
+    ZkpServeTableSet sets[ZKP_SERVE_MAX_SETS];
 } ZkpServeConfig;
 
 typedef struct ZkpProverRequest {
@@ -58,7 +76,8 @@ typedef struct ZkpServeStats {
 } ZkpServeStats;
 
 /* bases_d: msm_tables tables of n_bases affine points resident on the current device
- * (n_bases >= 2^max_k), e.g. built by zkp_msm_precompute_device. */
+ * (n_bases >= 2^max_k), e.g. built by zkp_msm_precompute_device; or null with n_sets > 0 (a
+ * window and table count tuned per size range). */
 cudaError_t zkp_serve_create(const ZkpServeConfig *cfg, const unsigned int *bases_d, unsigned long long n_bases,
                              ZkpServer **out);
 /* Non-blocking; returns a ticket >= 0.  A malformed request (k outside [min_k, max_k]) or one

@@ -146,3 +146,23 @@ def test_per_call_path_matches_served(zk, bases):
         srv.close()
     words, summary = zk.serving.run_schedule_per_call(prover, [(0.0, 10, 41), (0.01, 11, 44)])
     assert summary["ok"] == 2 and summary["p99_ms"] >= summary["p50_ms"] > 0
+
+
+def test_per_size_table_sets(zk, bases):
+    """A server with two resident table sets (different windows and table counts by size)
+    returns the same results as one with a single untabled set."""
+    sets = [(zk.msm.ResidentBases(bases[: 1 << 12], window=9, n_tables=29), 12),
+            (zk.msm.ResidentBases(bases, window=10, n_tables=26), MAX_K)]
+    a = zk.serving.Server(sets, hbm_bytes=4 << 30, max_inflight=3, ext_log=2, min_k=MIN_K, max_k=MAX_K)
+    b = server(zk, bases, 1)
+    try:
+        reqs = [(10, 61), (12, 62), (13, 63), (14, 64)]
+        ta = [a.submit(k, s) for k, s in reqs]
+        tb = [b.submit(k, s) for k, s in reqs]
+        for x, y in zip(ta, tb):
+            ra, rb = a.wait(x), b.wait(y)
+            assert ra.status == 0 and rb.status == 0
+            assert np.array_equal(zk.serving.result_words(ra), zk.serving.result_words(rb))
+    finally:
+        a.close()
+        b.close()

@@ -486,23 +486,42 @@ inline u32 digit_cap(u32 L) {
     return d ? d : MAX_D;
 }
 
-inline Plan make_plan(u32 L) {
+// Balanced split of L bits into passes of at most `cap` bits, top digit first, written into
+// p starting at pass `first` with the digits below bit `top`.
+inline void split_digits(Plan &p, u32 first, u32 L, u32 cap) {
+    const u32 np = (L + cap - 1) / cap;
+    const u32 base = L / np, extra = L % np;
+    u32 rem = L;
+    for (u32 i = 0; i < np; i++) {
+        p.D[first + i] = base + (i < extra ? 1 : 0);
+        rem -= p.D[first + i];
+        p.lo[first + i] = rem;
+    }
+    p.np = first + np;
+}
+
+// Plan for 2^L elements.  The tuned digit cap applies to plain table-mode transforms.  A
+// transform whose first pass multiplies by a coset shift or reads a shorter source keeps that
+// pass at up to MAX_D bits: the first pass builds per-pencil shift tables, and the cost of
+// that set-up grows with the number of pencils.  Recompute mode (roots rebuilt per pencil) and
+// the batched form (one shared-memory pencil kernel for every pass) ignore the cap.
+inline Plan make_plan(u32 L, bool wide_first = false, bool ignore_cap = false) {
     Plan p{};
-    const u32 cap = digit_cap(L);
-    if (L <= cap) {
+    const u32 cap = ignore_cap ? MAX_D : digit_cap(L);
+    const u32 first_cap = wide_first ? (cap > MAX_D ? cap : MAX_D) : cap;
+    if (L <= first_cap) {
         p.np = 1;
         p.D[0] = L;
         p.lo[0] = 0;
         return p;
     }
-    p.np = (L + cap - 1) / cap;
-    u32 base = L / p.np, extra = L % p.np;
-    u32 rem = L;
-    for (u32 i = 0; i < p.np; i++) {
-        p.D[i] = base + (i < extra ? 1 : 0);
-        rem -= p.D[i];
-        p.lo[i] = rem;
+    if (!wide_first || first_cap == cap) {
+        split_digits(p, 0, L, cap);
+        return p;
     }
+    p.D[0] = first_cap;
+    p.lo[0] = L - first_cap;
+    split_digits(p, 1, L - first_cap, cap);
     return p;
 }
 
@@ -550,7 +569,7 @@ cudaError_t launch_pass(const PassArgs &a, cudaStream_t stream) {
 // Runs the full plan.  src (if non-null) is the pass-0 source for the coset LDE.
 cudaError_t run(const View &v, const View *src, u64 src_len, u32 L, const u32 *tw, const u32 *omegas,
                 const u32 *shift, const u32 *scale, cudaStream_t stream) {
-    const Plan plan = make_plan(L);
+    const Plan plan = make_plan(L, shift != nullptr || src != nullptr, omegas != nullptr);
     profiler().begin(stream);
     for (u32 p = 0; p < plan.np; p++) {
         PassArgs a{};
@@ -673,7 +692,7 @@ extern "C" cudaError_t zkp_ntt_batch_plan_create(const ZkpNttTask *tasks, unsign
             delete plan;
             return cudaErrorInvalidValue;
         }
-        const ntt::Plan p = ntt::make_plan(L);
+        const ntt::Plan p = ntt::make_plan(L, task.shift_d != nullptr, /*ignore_cap=*/true);
         for (u32 ph = 0; ph < p.np; ph++) {
             if (args.size() <= ph) {
                 args.emplace_back();

@@ -127,8 +127,13 @@ using FusedFn = cudaError_t (*)(const ConstPolyPtr *, const PolyPtr *, unsigned 
 struct ZkpServer {
     ZkpServeConfig cfg{};
     int device = 0;
-    const u32 *bases = nullptr;
-    u64 n_bases = 0;
+    std::vector<ZkpServeTableSet> sets;  // by ascending max_k
+
+    const ZkpServeTableSet &set_for(u32 k) const {
+        for (const auto &t : sets)
+            if (k <= t.max_k) return t;
+        return sets.back();
+    }
     Arena arena;
     std::vector<SizeConsts> consts;  // index k
     u32 *shift = nullptr;            // coset shift 7 (Montgomery)
@@ -182,9 +187,10 @@ bool plan_request(ZkpServer *s, u32 k, Plan *p) {
     p->args = take(8 * sizeof(PolyPtr));
     p->results = take(4 * 64 + 2 * 32);
     ZkpMsmTask t[4];
+    const ZkpServeTableSet &ts = s->set_for(k);
     for (int i = 0; i < 4; i++)
-        t[i] = ZkpMsmTask{s->bases, s->cfg.msm_tables, s->bases /*sizes only*/, n, s->cfg.msm_window,
-                          reinterpret_cast<u32 *>(16), s->n_bases};
+        t[i] = ZkpMsmTask{ts.tables_d, ts.n_tables, ts.tables_d /*sizes only*/, n, ts.window,
+                          reinterpret_cast<u32 *>(16), ts.rows};
     p->msm_ws_bytes = (unsigned long)zkp_msm_batch_workspace_size(t, 4);
     if (p->msm_ws_bytes == 0) return false;
     p->msm_ws = take(p->msm_ws_bytes);
@@ -238,13 +244,14 @@ cudaError_t launch_program(ZkpServer *s, Request *r, ZkpServer::Slot &slot) {
     RUN(cudaMemcpyAsync(P(p.args), stage, 7 * sizeof(PolyPtr), cudaMemcpyHostToDevice, st));
     const PolyPtr *dargs = reinterpret_cast<const PolyPtr *>(P(p.args));
     RUN(s->fused(reinterpret_cast<const ConstPolyPtr *>(dargs), dargs + 6, N, true, nullptr, st));
-    // four MSMs over the resident bases in one batched launch set
-    const u32 nt = s->cfg.msm_tables, w = s->cfg.msm_window;
+    // four MSMs over the resident bases of this size's table set in one batched launch set
+    const ZkpServeTableSet &ts = s->set_for(k);
+    const u32 nt = ts.n_tables, w = ts.window;
     ZkpMsmTask t[4] = {
-        {s->bases, nt, P(p.a), n, w, P(p.results) + 0, s->n_bases},
-        {s->bases, nt, P(p.b), n, w, P(p.results) + 16, s->n_bases},
-        {s->bases, nt, P(p.c), n, w, P(p.results) + 32, s->n_bases},
-        {s->bases, nt, P(p.q), n, w, P(p.results) + 48, s->n_bases},
+        {ts.tables_d, nt, P(p.a), n, w, P(p.results) + 0, ts.rows},
+        {ts.tables_d, nt, P(p.b), n, w, P(p.results) + 16, ts.rows},
+        {ts.tables_d, nt, P(p.c), n, w, P(p.results) + 32, ts.rows},
+        {ts.tables_d, nt, P(p.q), n, w, P(p.results) + 48, ts.rows},
     };
     RUN(zkp_msm_batch(t, 4, P(p.msm_ws), p.msm_ws_bytes, st));
     // two evaluations
@@ -352,16 +359,28 @@ extern "C" unsigned long long zkp_serve_footprint(const ZkpServer *s, unsigned i
 
 extern "C" cudaError_t zkp_serve_create(const ZkpServeConfig *cfg, const unsigned int *bases_d,
                                         unsigned long long n_bases, ZkpServer **out) {
-    if (!cfg || !out || !bases_d || cfg->max_inflight == 0 || cfg->msm_tables == 0 ||
-        (cfg->msm_tables > 1 && cfg->msm_window == 0) || cfg->min_k < 1 || cfg->max_k > 26 ||
-        cfg->min_k > cfg->max_k || cfg->ext_log < 1 || cfg->ext_log > 3 || n_bases < (1ull << cfg->max_k))
+    if (!cfg || !out || cfg->max_inflight == 0 || cfg->min_k < 1 || cfg->max_k > 26 || cfg->min_k > cfg->max_k ||
+        cfg->ext_log < 1 || cfg->ext_log > 3 || cfg->n_sets > ZKP_SERVE_MAX_SETS)
         return cudaErrorInvalidValue;
+    std::vector<ZkpServeTableSet> sets;
+    if (cfg->n_sets == 0) {
+        sets.push_back(ZkpServeTableSet{bases_d, n_bases, cfg->msm_window, cfg->msm_tables, cfg->max_k});
+    } else {
+        sets.assign(cfg->sets, cfg->sets + cfg->n_sets);
+    }
+    for (size_t i = 0; i < sets.size(); i++) {
+        const ZkpServeTableSet &t = sets[i];
+        const u32 kmax = t.max_k < cfg->max_k ? t.max_k : cfg->max_k;
+        if (!t.tables_d || t.n_tables == 0 || (t.n_tables > 1 && t.window == 0) || t.rows < (1ull << kmax) ||
+            (i > 0 && t.max_k <= sets[i - 1].max_k))
+            return cudaErrorInvalidValue;
+    }
+    if (sets.back().max_k < cfg->max_k) return cudaErrorInvalidValue;
     auto *s = new ZkpServer();
     s->cfg = *cfg;
     s->t0 = std::chrono::steady_clock::now();
     cudaGetDevice(&s->device);
-    s->bases = bases_d;
-    s->n_bases = n_bases;
+    s->sets = sets;
     // fused quotient kernel, generated next to this library (lib/fused/)
     Dl_info info;
     std::string dir = ".";

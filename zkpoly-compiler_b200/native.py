@@ -117,10 +117,19 @@ class ZkpMsmTask(ctypes.Structure):
                 ("table_stride", ctypes.c_ulonglong)]
 
 
+class ZkpServeTableSet(ctypes.Structure):
+    _fields_ = [("tables_d", ctypes.c_void_p), ("rows", ctypes.c_ulonglong), ("window", ctypes.c_uint),
+                ("n_tables", ctypes.c_uint), ("max_k", ctypes.c_uint)]
+
+
+ZKP_SERVE_MAX_SETS = 8
+
+
 class ZkpServeConfig(ctypes.Structure):
     _fields_ = [("hbm_bytes", ctypes.c_ulonglong), ("max_inflight", ctypes.c_uint), ("ext_log", ctypes.c_uint),
                 ("min_k", ctypes.c_uint), ("max_k", ctypes.c_uint), ("msm_window", ctypes.c_uint),
-                ("msm_tables", ctypes.c_uint)]
+                ("msm_tables", ctypes.c_uint), ("n_sets", ctypes.c_uint),
+                ("sets", ZkpServeTableSet * ZKP_SERVE_MAX_SETS)]
 
 
 class ZkpProverRequest(ctypes.Structure):

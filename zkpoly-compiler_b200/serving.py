@@ -10,7 +10,8 @@ import time
 import numpy as np
 import torch
 
-from .native import (ZkpProverRequest, ZkpProverResult, ZkpServeConfig, ZkpServeStats, check, load)
+from .native import (ZkpProverRequest, ZkpProverResult, ZkpServeConfig, ZkpServeStats, ZkpServeTableSet, check,
+                     load)
 from .scalar import require_cuda
 
 LIB = "libzkp_runtime.so"
@@ -19,16 +20,25 @@ LIB = "libzkp_runtime.so"
 class Server:
     def __init__(self, bases, hbm_bytes: int, max_inflight: int = 8, ext_log: int = 2,
                  min_k: int = 14, max_k: int = 22, msm_window: int = 0):
-        """bases: a (N, 16) int32 device tensor of affine points, or a msm.ResidentBases
-        (its precomputed tables and window are used)."""
+        """bases: a (N, 16) int32 device tensor of affine points, a msm.ResidentBases (its
+        precomputed tables and window are used for every size), or a list of
+        (msm.ResidentBases, max_k) by ascending max_k (per-size table sets, see resident_sets)."""
         require_cuda()
         self.lib = load(LIB)
         self.bases = bases
-        if hasattr(bases, "tables"):
+        n_sets, sets = 0, []
+        if isinstance(bases, (list, tuple)):
+            ptr, n_bases, tables = None, 0, 1
+            for rb, mk in bases:
+                sets.append(ZkpServeTableSet(rb.tables.data_ptr(), rb.n, rb.window, rb.n_tables, mk))
+            n_sets = len(sets)
+        elif hasattr(bases, "tables"):
             ptr, n_bases, tables, msm_window = bases.tables.data_ptr(), bases.n, bases.n_tables, bases.window
         else:
             ptr, n_bases, tables = bases.data_ptr(), bases.shape[0], 1
-        cfg = ZkpServeConfig(hbm_bytes, max_inflight, ext_log, min_k, max_k, msm_window, tables)
+        cfg = ZkpServeConfig(hbm_bytes, max_inflight, ext_log, min_k, max_k, msm_window, tables, n_sets)
+        for i, t in enumerate(sets):
+            cfg.sets[i] = t
         self.h = ctypes.c_void_p()
         check(self.lib.zkp_serve_create(ctypes.byref(cfg), ptr, n_bases, ctypes.byref(self.h)), "zkp_serve_create")
 
@@ -66,6 +76,22 @@ class Server:
         self.close()
 
 
+def resident_sets(points: torch.Tensor, k_lo: int, k_hi: int):
+    """Per-size resident table sets for a server: sizes 2^k_lo .. 2^k_hi grouped by the tuned
+    (window, tables) of each size, one msm.ResidentBases per group over the first 2^(largest k)
+    points.  Returns [(ResidentBases, max_k)] by ascending max_k."""
+    from . import msm, tuner
+    groups = []
+    for k in range(k_lo, k_hi + 1):
+        cfg = tuner.msm_resident_config(1 << k)
+        if groups and groups[-1][0] == cfg:
+            groups[-1][1] = k
+        else:
+            groups.append([cfg, k])
+    assert len(groups) <= 8, "too many table sets"
+    return [(msm.ResidentBases(points[: 1 << mk], window=c, n_tables=nt), mk) for (c, nt), mk in groups]
+
+
 class PerCallProver:
     """The plain per-call path: the served program (include/zkp_runtime.h), one request at a
     time, every operator called through its own per-call entry point on one stream.  The four
@@ -77,6 +103,8 @@ class PerCallProver:
     def __init__(self, bases, ext_log: int = 2, device="cuda", max_k: int | None = None):
         from . import msm
         require_cuda()
+        if isinstance(bases, (list, tuple)):
+            bases = bases[-1][0]  # the set that covers the largest size holds every base
         pts = bases.tables[: bases.n] if hasattr(bases, "tables") else bases
         # host point table (pinned, as a runtime's host pool would hand it out)
         self.h_bases = pts.cpu().pin_memory()
