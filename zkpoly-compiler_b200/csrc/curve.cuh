@@ -12,16 +12,15 @@
 namespace zk {
 
 // The curve formulas reach the Fq product and square through fmul / fsqr.  By default they are
-// inlined.  With ZK_CURVE_OUTLINE_MUL they call one out-of-line copy each, which keeps a loop
-// of additions inside the instruction cache at the price of a call per product.  On B200 the
-// out-of-line form was 11 % faster for the 2^22 MSM while the product ran one low chain and
-// one high chain per row; with the paired product (smaller code) the inlined form is 7 %
-// faster (16.0 vs 17.2 ms, same results).
+// inlined.  With ZK_CURVE_OUTLINE_MUL both call one out-of-line product, which keeps a loop of
+// additions inside the instruction cache at the price of a call (and register traffic) per
+// product.  On B200 the out-of-line form was 11 % faster for the 2^22 MSM while the product
+// ran one low chain and one high chain per row; with the paired product the inlined form is
+// faster (15.7 vs 17.9 ms, same results).
 #ifdef ZK_CURVE_OUTLINE_MUL
 static __device__ __noinline__ Fq fq_mul_call(const Fq a, const Fq b) { return Fq::mul(a, b); }
-static __device__ __noinline__ Fq fq_sqr_call(const Fq a) { return Fq::sqr(a); }
 ZK_DI Fq fmul(const Fq &a, const Fq &b) { return fq_mul_call(a, b); }
-ZK_DI Fq fsqr(const Fq &a) { return fq_sqr_call(a); }
+ZK_DI Fq fsqr(const Fq &a) { return fq_mul_call(a, a); }
 #else
 ZK_DI Fq fmul(const Fq &a, const Fq &b) { return Fq::mul(a, b); }
 ZK_DI Fq fsqr(const Fq &a) { return Fq::sqr(a); }

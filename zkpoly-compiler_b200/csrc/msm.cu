@@ -371,26 +371,29 @@ __global__ void __launch_bounds__(256, ZK_ACC_MIN_BLOCKS) accumulate_kernel(cons
     u32 cur = sorted_bucket[start];
     const u32 *pts = b.task[find_task(b.key_first, b.ntasks, (u64)cur)].points;
     G1X acc = G1X::from_affine(fetch_point(pts, sorted_point[start]));
-    // The point of the next entry is always in flight while the current one is added: its
-    // load is issued one iteration ahead and its sign applied only when it is used.
+    // The next record's bucket, code and point address are read one iteration ahead; its point
+    // is loaded when it is used.  (Keeping the point load itself one iteration ahead helped
+    // while the Fq product was slower; with the paired product the 16 registers it holds cost
+    // more: 16.0 vs 15.7 ms at 2^22.)
     u32 nbk = EMPTY, ncode = 0;
     const u32 *npts = pts;
-    G1A nxt;
+    const u32 *naddr = pts;
     if (start + 1 < end) {
         nbk = sorted_bucket[start + 1];
         ncode = sorted_point[start + 1];
         if (nbk != cur) npts = b.task[find_task(b.key_first, b.ntasks, (u64)nbk)].points;
-        nxt = G1A::load_nc(npts + (u64)(ncode & 0x7fffffffu) * 16);
+        naddr = npts + (u64)(ncode & 0x7fffffffu) * 16;
     }
     for (u64 p = start + 1; p <= end; p++) {
         const u32 bk = nbk, code = ncode;
         const u32 *bpts = npts;
-        G1A pt = nxt;
+        G1A pt;
+        if (p < end) pt = G1A::load_nc(naddr);
         if (p + 1 < end) {
             nbk = sorted_bucket[p + 1];
             ncode = sorted_point[p + 1];
             if (nbk != bk) npts = b.task[find_task(b.key_first, b.ntasks, (u64)nbk)].points;
-            nxt = G1A::load_nc(npts + (u64)(ncode & 0x7fffffffu) * 16);
+            naddr = npts + (u64)(ncode & 0x7fffffffu) * 16;
         } else {
             nbk = EMPTY;
         }
