@@ -506,9 +506,9 @@ def emit(args, zk, rank, world, n_msm, n_ntt, ntt_ms, msm_ms, step_ms, pass_ms, 
                                f"2^{NTT_LOG} NTT)", "bound": "hbm",
                      "achieved": ntt_bytes_per_pass / (pass_avg / 1e3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
                      "frac": ntt_bytes_per_pass / (pass_avg / 1e3) / 1e9 / hbm_peak, "peak_source": peak_kind,
-                     # ncu DRAM bytes per pass launch: 61.9 B per element at 2^22 (three tuned
-                     # passes, 778 MB), scaled by the element count
-                     "traffic": 61.9 * n_ntt,
+                     # ncu DRAM bytes per pass launch: 58.7 B per element at 2^22 (four register
+                     # passes, 985 MB), scaled by the element count
+                     "traffic": 58.7 * n_ntt,
                      "note": "IMAD-bound kernel: HBM fraction reported as asked; see int_roofline"},
         "int_roofline": {
             # denominator: Montgomery products per second of the library's own product routine
