@@ -184,6 +184,7 @@ class NttBatch:
             self._keep += [x, tw, sh, sc]
             arr[i] = ZkpNttTask(x.poly_ptr(), tw.values.data_ptr(), log_n, _ptr(sh), _ptr(sc))
         self._plan = ctypes.c_void_p()
+        self._destroy = lib.zkp_ntt_batch_plan_destroy  # kept: module globals may be gone at exit
         check(lib.zkp_ntt_batch_plan_create(ctypes.cast(arr, ctypes.c_void_p), len(tasks),
                                             ctypes.byref(self._plan)), "zkp_ntt_batch_plan_create")
 
@@ -192,7 +193,7 @@ class NttBatch:
 
     def __del__(self):
         if getattr(self, "_plan", None):
-            load(LIB).zkp_ntt_batch_plan_destroy(self._plan)
+            self._destroy(self._plan)
             self._plan = None
 
 
