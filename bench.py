@@ -35,6 +35,18 @@ def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
 
+def max_over_ranks(values, device=None):
+    """Element-wise maximum of per-rank timings over all ranks (the job's time is its slowest
+    rank's); the identity on one process.  Works on any initialised backend (nccl, gloo)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return list(values)
+    t = torch.tensor(list(values), dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
 def peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -221,9 +233,7 @@ def run_gpu(args):
     msm_ms = ev[1].elapsed_time(ev[2]) / args.steps
     step_ms = ntt_ms + msm_ms
     if world > 1:
-        t = torch.tensor([ntt_ms, msm_ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ntt_ms, msm_ms = t.tolist()
+        ntt_ms, msm_ms = max_over_ranks([ntt_ms, msm_ms], dev)
         step_ms = ntt_ms + msm_ms
 
     # ---- per-kernel timing from the libraries' own stream events (separate, untimed runs)
