@@ -48,6 +48,13 @@ cudaError_t batched_invert(void *temp_buffer, unsigned long *buffer_size, PolyPt
 cudaError_t inv_scalar(unsigned int *target, cudaStream_t stream);
 cudaError_t scalar_pow(unsigned int *target, unsigned long long exp, cudaStream_t stream);
 
+/* lookup permutation over the first `usable` rows (poly.h:28, permute.cuh:74-222): res_input =
+ * input sorted ascending by canonical value; res_table = at the first row of each run of equal
+ * values that value (taken once from the table), elsewhere the unused table values ascending.
+ * Every input value must occur in the table.  temp_buffer == null: *buffer_size = bytes needed. */
+cudaError_t permute(void *temp_buffer, unsigned long *buffer_size, unsigned long usable, ConstPolyPtr input,
+                    ConstPolyPtr table, PolyPtr res_input, PolyPtr res_table, cudaStream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -9,6 +9,9 @@ xmake / Makefile.msm, is not used):
   libref_msm_<s>_<t>.so    core/src/msm/src/msm.cu with MSM_WINDOW_SIZE = s and
                            MSM_TARGET_WINDOWS = t (the per-configuration library the reference
                            builds, Makefile.msm), MSM_BITS 254, curve bn254, debug off
+  libref_poly.so           core/src/poly/src/*.cu (poly_basic, poly_eval, kate_division,
+                           scan_mul, batched_invert, permute) with POLY_FIELD = bn254_fr::Element;
+                           each source compiled to an object in parallel, then linked
 
 Skipped when the checkout is absent; the built libraries travel with the repository snapshot.
 The GPU libraries serve the parity tests that run the reference's kernels next to this
@@ -51,6 +54,49 @@ def jobs():
     return out
 
 
+POLY_SOURCES = ["poly_basic", "poly_eval", "kate_division", "scan_mul", "batched_invert", "permute"]
+
+
+def poly_objects():
+    """(object, source, command) for each reference poly source."""
+    src_dir = os.path.join(REF, "core/src/poly/src")
+    obj_dir = os.path.join(OUT_DIR, "obj")
+    out = []
+    for name in POLY_SOURCES:
+        src = os.path.join(src_dir, name + ".cu")
+        obj = os.path.join(obj_dir, name + ".o")
+        cmd = [NVCC, "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-c", "-gencode", "arch=compute_100a,code=sm_100a",
+               "--extended-lambda", "-diag-suppress", "550,177", "-DPOLY_FIELD=bn254_fr::Element", src]
+        out.append((obj, src, cmd))
+    return out
+
+
+def build_poly(failed):
+    target = os.path.join(OUT_DIR, "libref_poly.so")
+    objs = poly_objects()
+    srcs = [src for _, src, _ in objs]
+    if os.path.exists(target) and all(os.path.getmtime(target) > os.path.getmtime(s) for s in srcs):
+        return
+    os.makedirs(os.path.join(OUT_DIR, "obj"), exist_ok=True)
+    procs = [(obj, subprocess.Popen(cmd + ["-o", obj], stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True))
+             for obj, _, cmd in objs]
+    ok = True
+    for obj, proc in procs:
+        log, _ = proc.communicate()
+        if proc.returncode != 0:
+            failed.append(f"{obj}:\n{log}")
+            ok = False
+    if not ok:
+        return
+    link = subprocess.run([NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", target + ".tmp",
+                           *[obj for obj, _, _ in objs]], capture_output=True, text=True)
+    if link.returncode != 0:
+        failed.append(f"{target}:\n{link.stderr}")
+        return
+    os.replace(target + ".tmp", target)
+    print(target)
+
+
 def main():
     if not os.path.isdir(REF):
         print("reference checkout absent; oracle/_ref not built")
@@ -63,6 +109,7 @@ def main():
         running.append((target, subprocess.Popen(cmd + ["-o", target + ".tmp"], stdout=subprocess.PIPE,
                                                  stderr=subprocess.STDOUT, text=True)))
     failed = []
+    build_poly(failed)
     for target, proc in running:
         log, _ = proc.communicate()
         if proc.returncode != 0:

@@ -324,3 +324,32 @@ def naive_msm(scalars: np.ndarray, bases: np.ndarray) -> np.ndarray:
     r = zeros(1, 8)
     lib().or_naive_msm(_p(r), _p(scalars), _p(bases), ctypes.c_size_t(len(scalars)))
     return r[0]
+
+
+def permute(inp: np.ndarray, table: np.ndarray, usable: int):
+    """Lookup permutation (restates the expected output of core/tests/poly.rs:569-700, the
+    contract of core/src/poly/src/permute.cuh:74-222).  Over the first `usable` rows: the input
+    sorted ascending by canonical value; for the table, the first row of each run of equal input
+    values holds that value (one occurrence removed from the table multiset), the other rows the
+    remaining table values, ascending.  Montgomery (n, 4) uint64 in and out."""
+    a_vals = sorted(limbs_to_int(from_mont(r)) for r in inp[:usable])
+    left = {}
+    for r in table[:usable]:
+        v = limbs_to_int(from_mont(r))
+        left[v] = left.get(v, 0) + 1
+    out_t = [None] * usable
+    repeated = []
+    for i, v in enumerate(a_vals):
+        if i == 0 or v != a_vals[i - 1]:
+            assert left.get(v, 0) > 0, "input value missing from the table"
+            left[v] -= 1
+            out_t[i] = v
+        else:
+            repeated.append(i)
+    rest = sorted(v for v, c in left.items() for _ in range(c))
+    assert len(rest) == len(repeated)
+    for i, v in zip(repeated, rest):
+        out_t[i] = v
+    pi = np.stack([to_mont(int_to_limbs(v)).reshape(4) for v in a_vals])
+    pt = np.stack([to_mont(int_to_limbs(v)).reshape(4) for v in out_t])
+    return pi, pt

@@ -49,3 +49,27 @@ def u32_to_u64(v):
 
 def u32_to_int(v):
     return sum(int(x) << (32 * i) for i, x in enumerate(v))
+
+
+def lookup_case(zk, n, usable, seed):
+    """A lookup instance shaped like the reference's permute test (core/tests/poly.rs:569-625):
+    table values uniform below 2n, inputs drawn from the distinct values of the table's usable
+    rows; returned as Montgomery device arrays (converted on the device by multiplying the
+    canonical values by R^2)."""
+    import torch
+    rng = np.random.default_rng(seed)
+    table = rng.integers(0, 2 * n, n, dtype=np.uint64)
+    distinct = np.unique(table[:usable])
+    inp = distinct[rng.integers(0, len(distinct), n)]
+    # raw words of R^2 mod r (the Montgomery form of R): multiplying by it maps x to x * R
+    r2 = np.array(zk.field.mont_words((1 << 256) % zk.field.FR_MODULUS), dtype=np.uint32)
+    out = []
+    for vals in (inp, table):
+        limbs = np.zeros((n, 8), dtype=np.uint32)
+        limbs[:, 0] = vals.astype(np.uint32)
+        arr = zk.ScalarArray.from_numpy(limbs)
+        powers = zk.ScalarArray.from_numpy(r2.reshape(1, 8))
+        zk.ntt.distribute_powers(arr, powers)
+        out.append(arr)
+    torch.cuda.synchronize()
+    return out

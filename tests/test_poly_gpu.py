@@ -1,6 +1,8 @@
 """Poly library on the GPU through the C ABI, bit-exact against the oracle / big integers."""
 import numpy as np
 import pytest
+
+from conftest import lookup_case
 import torch
 
 pytestmark = pytest.mark.gpu
@@ -140,3 +142,15 @@ def test_square_matches_mul(zk, orc):
     r = zk.ScalarArray.zeros(n)
     zk.poly.poly_square(r, dev(zk, a))
     assert np.array_equal(r.numpy_u64(), orc.vec_mul(a, a))
+
+
+@pytest.mark.parametrize("log_n", [6, 10, 14])
+def test_permute_matches_oracle(zk, orc, log_n):
+    n = 1 << log_n
+    usable = n - min(25, n // 4)
+    inp, table = lookup_case(zk, n, usable, 70 + log_n)
+    ri, rt = zk.ScalarArray.alloc(usable), zk.ScalarArray.alloc(usable)
+    zk.poly.permute(inp, table, usable, ri, rt)
+    ei, et = orc.permute(inp.numpy_u64(), table.numpy_u64(), usable)
+    assert np.array_equal(ri.numpy_u64(), ei)
+    assert np.array_equal(rt.numpy_u64(), et)

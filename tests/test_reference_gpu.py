@@ -1,6 +1,7 @@
 """The reference's own CUDA kernels, built from its sources into oracle/_ref (oracle/build_ref.py),
-run next to this repository's kernels on the same inputs: NTT (ssip_ntt) and MSM (msm, two of the
-reference's library configurations) must agree bit for bit.  Skipped when oracle/_ref was not
+run next to this repository's kernels on the same inputs: NTT (ssip_ntt), MSM (msm, two of the
+reference's library configurations) and the poly library (permute, poly_eval, batched_invert,
+kate_division, scan_mul) must agree bit for bit.  Skipped when oracle/_ref was not
 built (no reference checkout where the libraries were built).
 
 With ZKP_REF_TIMING=1 the tests also time both sides (CUDA events for the NTT, host clock for
@@ -158,3 +159,103 @@ def test_reference_msm_precomputed_matches(zk, log_n):
         print(json.dumps({"compare": "msm host-buffer ABI", "log_n": log_n, "reference_s17_t8_ms": dt_ref * 1e3,
                           "this_abi_ms": min(dt) * 1e3, "this_resident_ms": e0.elapsed_time(e1) / 5,
                           "resident_config": [c, nt]}))
+
+
+def test_reference_permute_matches(zk):
+    """permute at 2^20 rows (24 + 1 blinding rows unused, as in the reference's test) against the
+    reference's own CUB-based permute."""
+    from conftest import lookup_case
+    ref = _ref_lib("libref_poly.so")
+    ref.permute.restype = ctypes.c_int
+    ref.permute.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_ulong), ctypes.c_ulong, zk.native.PolyPtr,
+                            zk.native.PolyPtr, zk.native.PolyPtr, zk.native.PolyPtr, ctypes.c_void_p]
+    n = 1 << 20
+    usable = n - 25
+    inp, table = lookup_case(zk, n, usable, 5)
+    outs = [zk.ScalarArray.alloc(usable) for _ in range(4)]
+    size = ctypes.c_ulong(0)
+    st = torch.cuda.current_stream().cuda_stream
+    assert ref.permute(None, ctypes.byref(size), usable, inp.poly_ptr(), table.poly_ptr(), outs[0].poly_ptr(),
+                       outs[1].poly_ptr(), st) == 0
+    tmp = torch.empty(size.value, dtype=torch.uint8, device="cuda")
+    run_ref = lambda: ref.permute(tmp.data_ptr(), ctypes.byref(size), usable, inp.poly_ptr(), table.poly_ptr(),
+                                  outs[0].poly_ptr(), outs[1].poly_ptr(), st)
+    assert run_ref() == 0
+    zk.poly.permute(inp, table, usable, outs[2], outs[3])
+    torch.cuda.synchronize()
+    assert torch.equal(outs[0].values, outs[2].values)
+    assert torch.equal(outs[1].values, outs[3].values)
+    if TIMING:
+        def t(fn, reps=5):
+            fn()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(reps):
+                fn()
+            e1.record()
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1) / reps
+        ms_ref = t(run_ref)
+        ms = t(lambda: zk.poly.permute(inp, table, usable, outs[2], outs[3]))
+        print(json.dumps({"compare": "permute", "rows": usable, "reference_ms": ms_ref, "this_ms": ms,
+                          "speedup": ms_ref / ms}))
+
+
+def _ref_poly(zk):
+    lib = _ref_lib("libref_poly.so")
+    P, V, UL = zk.native.PolyPtr, ctypes.c_void_p, ctypes.POINTER(ctypes.c_ulong)
+    for name, args in (("poly_eval", [V, UL, P, V, V, V]), ("batched_invert", [V, UL, P, V]),
+                       ("kate_division", [V, UL, ctypes.c_uint, P, V, P, V]), ("scan_mul", [V, UL, P, V])):
+        getattr(lib, name).restype = ctypes.c_int
+        getattr(lib, name).argtypes = args
+    return lib
+
+
+def _temp_for(fn, *args):
+    size = ctypes.c_ulong(0)
+    assert fn(None, ctypes.byref(size), *args) == 0
+    return torch.empty(max(size.value, 1), dtype=torch.uint8, device="cuda"), size
+
+
+@pytest.mark.parametrize("log_n", [10, 20])
+def test_reference_poly_library_matches(zk, log_n):
+    """poly_eval, batched_invert (with zeros), kate_division and scan_mul against the reference's
+    own kernels on the same inputs."""
+    ref = _ref_poly(zk)
+    n = 1 << log_n
+    st = torch.cuda.current_stream().cuda_stream
+    p = zk.ScalarArray(zk.gen.fr(800 + log_n, n))
+    x = zk.gen.fr(801, 1)
+    # poly_eval
+    res_ref = torch.zeros(8, dtype=torch.int32, device="cuda")
+    res = torch.zeros(8, dtype=torch.int32, device="cuda")
+    tmp, size = _temp_for(ref.poly_eval, p.poly_ptr(), None, None, None)
+    assert ref.poly_eval(tmp.data_ptr(), ctypes.byref(size), p.poly_ptr(), res_ref.data_ptr(), x.data_ptr(), st) == 0
+    zk.poly.poly_eval(p, x, res)
+    torch.cuda.synchronize()
+    assert torch.equal(res_ref, res)
+    # batched_invert, every 7th element zero
+    v = p.values.clone()
+    v[::7] = 0
+    a_ref, a = zk.ScalarArray(v.clone()), zk.ScalarArray(v.clone())
+    tmp, size = _temp_for(ref.batched_invert, a_ref.poly_ptr(), None)
+    assert ref.batched_invert(tmp.data_ptr(), ctypes.byref(size), a_ref.poly_ptr(), st) == 0
+    zk.poly.batched_invert(a)
+    torch.cuda.synchronize()
+    assert torch.equal(a_ref.values, a.values)
+    # kate_division: q = p / (X - b), length n
+    q_ref, q = zk.ScalarArray.zeros(n), zk.ScalarArray.zeros(n)
+    tmp, size = _temp_for(ref.kate_division, log_n, p.poly_ptr(), None, q_ref.poly_ptr(), None)
+    assert ref.kate_division(tmp.data_ptr(), ctypes.byref(size), log_n, p.poly_ptr(), x.data_ptr(),
+                             q_ref.poly_ptr(), st) == 0
+    zk.poly.kate_division(p, x, q)
+    torch.cuda.synchronize()
+    assert torch.equal(q_ref.values, q.values)
+    # scan_mul (inclusive product scan in place)
+    s_ref, s_ = zk.ScalarArray(p.values.clone()), zk.ScalarArray(p.values.clone())
+    tmp, size = _temp_for(ref.scan_mul, s_ref.poly_ptr(), None)
+    assert ref.scan_mul(tmp.data_ptr(), ctypes.byref(size), s_ref.poly_ptr(), st) == 0
+    zk.poly.scan_mul(s_)
+    torch.cuda.synchronize()
+    assert torch.equal(s_ref.values, s_.values)

@@ -511,3 +511,4 @@ extern "C" cudaError_t kate_division(void *temp_buf, unsigned long *temp_buf_siz
     }
     return cudaSuccess;
 }
+#include "permute.cuh"

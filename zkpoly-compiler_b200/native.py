@@ -98,6 +98,8 @@ SIGNATURES = {
                                         PolyPtr, c_void_p]),
         "scan_mul": (cudaError_t, [c_void_p, ctypes.POINTER(ctypes.c_ulong), PolyPtr, c_void_p]),
         "batched_invert": (cudaError_t, [c_void_p, ctypes.POINTER(ctypes.c_ulong), PolyPtr, c_void_p]),
+        "permute": (cudaError_t, [c_void_p, ctypes.POINTER(ctypes.c_ulong), ctypes.c_ulong, PolyPtr, PolyPtr, PolyPtr,
+                                  PolyPtr, c_void_p]),
         "inv_scalar": (cudaError_t, [c_void_p, c_void_p]),
         "scalar_pow": (cudaError_t, [c_void_p, ctypes.c_ulonglong, c_void_p]),
     },

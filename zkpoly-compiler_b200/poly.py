@@ -103,6 +103,19 @@ def batched_invert(t: ScalarArray, stream=None):
           "batched_invert")
 
 
+def permute(inp: ScalarArray, table: ScalarArray, usable: int, res_input: ScalarArray, res_table: ScalarArray,
+            stream=None):
+    """Lookup permutation of the first `usable` rows (core/src/poly.rs PolyPermute, reference
+    permute.cuh:74-222): res_input = sorted input, res_table = the matching table arrangement."""
+    lib = _lib()
+    size = ctypes.c_ulong(0)
+    check(lib.permute(None, ctypes.byref(size), usable, inp.poly_ptr(), table.poly_ptr(), res_input.poly_ptr(),
+                      res_table.poly_ptr(), stream_handle(stream)), "permute(size query)")
+    temp = _temp(size.value, inp.values.device)
+    check(lib.permute(temp.data_ptr(), ctypes.byref(size), usable, inp.poly_ptr(), table.poly_ptr(),
+                      res_input.poly_ptr(), res_table.poly_ptr(), stream_handle(stream)), "permute")
+
+
 def inv_scalar(x: torch.Tensor, stream=None):
     check(_lib().inv_scalar(x.data_ptr(), stream_handle(stream)), "inv_scalar")
 
