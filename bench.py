@@ -285,6 +285,10 @@ def run_gpu(args):
     fused = measure_fused(zk, gen, dev, stream, hbm_peak=peaks()[0],
                           mont_peak=mont_per_s) if not args.no_fused else None
 
+    # ---- poly library rows (evaluation, batched inversion, division by X - b)
+    poly = measure_poly(zk, gen, dev, stream, hbm_peak=peaks()[0], mont_peak=mont_per_s) \
+        if not args.no_fused else None
+
     # ---- batched form (mixed NTT/MSM workload) and served form (Poisson arrivals)
     batched = measure_batched(zk, args) if (not args.no_batched and rank == 0) else None
     served = measure_served(zk, bases, args) if (not args.no_served and rank == 0) else None
@@ -300,7 +304,7 @@ def run_gpu(args):
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_reference(args.ref_msm_log, args.ref_ntt_log)
     emit(args, zk, rank, world, n_msm, n_ntt, ntt_ms, msm_ms, step_ms, pass_ms, bitrev_ms, stage_ms, imad_per_s,
-         e2e_msm_s, e2e_ntt_s, cpu, clocks, bases, batched, served, fused, mont_per_s)
+         e2e_msm_s, e2e_ntt_s, cpu, clocks, bases, batched, served, fused, mont_per_s, poly)
 
 
 def measure_fused(zk, gen, dev, stream, hbm_peak, mont_peak, log_n=NTT_LOG, ext=3, reps=10):
@@ -333,6 +337,48 @@ def measure_fused(zk, gen, dev, stream, hbm_peak, mont_peak, log_n=NTT_LOG, ext=
            "fr_mults_per_s": mults / (ms / 1e3), "mont_frac": mults / (ms / 1e3) / mont_peak,
            "bytes_per_elem": 160, "fr_mults_per_elem": 3}
     del a, b, c, z, q
+    torch.cuda.empty_cache()
+    return out
+
+
+def measure_poly(zk, gen, dev, stream, hbm_peak, mont_peak, log_n=22, reps=10):
+    """poly_eval, batched_invert and kate_division over 2^log_n elements (inputs larger than L2):
+    CUDA-event time per call, algorithmic bytes and Montgomery products per element as each
+    kernel's cost model below states."""
+    import torch
+    n = 1 << log_n
+    with torch.cuda.stream(stream):
+        p = zk.ScalarArray(gen.fr(900, n, dev))
+        x = gen.fr(901, 1, dev)
+        res = torch.zeros(8, dtype=torch.int32, device=dev)
+        inv = zk.ScalarArray(gen.fr(902, n, dev))
+        q = zk.ScalarArray.zeros(n, dev)
+    torch.cuda.synchronize()
+    # (name, call, algorithmic bytes per element, algorithmic products per element): Horner
+    # evaluation reads each coefficient once with one product; Montgomery's batched inversion
+    # reads and writes each element with three products; division by X - b reads p, writes q,
+    # one product per coefficient
+    cases = [
+        ("poly_eval", lambda: zk.poly.poly_eval(p, x, res, stream=stream), 32, 1),
+        ("batched_invert", lambda: zk.poly.batched_invert(inv, stream=stream), 64, 3),
+        ("kate_division", lambda: zk.poly.kate_division(p, x, q, stream=stream), 64, 1),
+    ]
+    out = {"n": n}
+    for name, call, bpe, mpe in cases:
+        for _ in range(2):
+            call()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            call()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        out[name] = {"ms": ms, "elems_per_s": n / (ms / 1e3), "bytes_per_elem": bpe,
+                     "hbm_frac": bpe * n / (ms / 1e3) / 1e9 / hbm_peak, "fr_mults_per_elem": mpe,
+                     "mont_frac": mpe * n / (ms / 1e3) / mont_peak}
+    del p, inv, q
     torch.cuda.empty_cache()
     return out
 
@@ -471,7 +517,8 @@ def run_e2e(zk, native, lib_msm, scalars, points, ntt_in, tw, stream, dev, local
 
 
 def emit(args, zk, rank, world, n_msm, n_ntt, ntt_ms, msm_ms, step_ms, pass_ms, bitrev_ms, stage_ms, imad_per_s,
-         e2e_msm_s, e2e_ntt_s, cpu, clocks, bases, batched=None, served=None, fused=None, mont_per_s=None):
+         e2e_msm_s, e2e_ntt_s, cpu, clocks, bases, batched=None, served=None, fused=None, mont_per_s=None,
+         poly=None):
     import torch
     if rank != 0:
         if world > 1:
@@ -542,6 +589,8 @@ def emit(args, zk, rank, world, n_msm, n_ntt, ntt_ms, msm_ms, step_ms, pass_ms, 
     }
     if fused:
         line["fused"] = fused
+    if poly:
+        line["poly"] = poly
     if batched:
         line["batched"] = batched
     if served:
