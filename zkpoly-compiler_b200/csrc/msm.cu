@@ -637,7 +637,11 @@ inline u32 grid_for(u64 items, u32 block, u32 per_sm = 8) {
 
 // Runs a batch of MSMs whose points / scalars are on the device; `ws` holds the layout
 // regions.  Launches only: no allocation, no host copy.
-cudaError_t run_batch(const Batch &b, const Layout &l, char *ws, cudaStream_t stream) {
+// points_ready (optional): the accumulation waits for it, so a host-to-device copy of the
+// points can overlap the digit sort.  scalars_read (optional): recorded once the scalars have
+// been read (after the scatter), so the caller may overwrite them.
+cudaError_t run_batch(const Batch &b, const Layout &l, char *ws, cudaStream_t stream,
+                      cudaEvent_t points_ready = nullptr, cudaEvent_t scalars_read = nullptr) {
     u32 *counts = reinterpret_cast<u32 *>(ws + l.counts);
     u32 *cursor = reinterpret_cast<u32 *>(ws + l.cursor);
     u32 *sb = reinterpret_cast<u32 *>(ws + l.sorted_bucket);
@@ -681,6 +685,8 @@ cudaError_t run_batch(const Batch &b, const Layout &l, char *ws, cudaStream_t st
         ZK_TRY(cudaGetLastError());
     }
     prof.mark("scatter", stream);
+    if (scalars_read) ZK_TRY(cudaEventRecord(scalars_read, stream));
+    if (points_ready) ZK_TRY(cudaStreamWaitEvent(stream, points_ready, 0));
     const u32 *live = counts + nb;
     if (l.chunks) {
         accumulate_kernel<<<(u32)((l.chunks + 255) / 256), 256, 0, stream>>>(b, sb, sp, live, bs, pp, pb, pf);
@@ -913,9 +919,11 @@ extern "C" cudaError_t zkp_msm_precompute_device(unsigned int *tables_d, unsigne
 }
 
 // device layout of one card's buffer for the reference ABI: points | scalars | result | batch ws
+// A card's buffer: the point tables, two scalar buffers (batch b uses buffer b % 2, so the next
+// batch's copy overlaps this batch's work), the result and the MSM workspace.
 struct CardLayout {
-    size_t points, scalars, result, ws, total;
-    msm::Batch batch;
+    size_t points, scalars[2], result, ws, total;
+    msm::Batch batch[2];
     msm::Layout l;
 };
 
@@ -924,16 +932,20 @@ static CardLayout card_layout(u64 cnt, u32 c, u32 nt, char *base) {
     size_t off = 0;
     cl.points = off;
     off += msm::align_up(cnt * nt * 64);
-    cl.scalars = off;
-    off += msm::align_up(cnt * 32);
+    for (int i = 0; i < 2; i++) {
+        cl.scalars[i] = off;
+        off += msm::align_up(cnt * 32);
+    }
     cl.result = off;
     off += 256;
     cl.ws = off;
     u32 *pts = base ? reinterpret_cast<u32 *>(base + cl.points) : nullptr;
-    u32 *sc = base ? reinterpret_cast<u32 *>(base + cl.scalars) : nullptr;
     u32 *res = base ? reinterpret_cast<u32 *>(base + cl.result) : nullptr;
-    cl.batch = msm::single(pts, nt, sc, cnt, c, res);
-    cl.l = msm::make_layout(cl.batch);
+    for (int i = 0; i < 2; i++) {
+        u32 *sc = base ? reinterpret_cast<u32 *>(base + cl.scalars[i]) : nullptr;
+        cl.batch[i] = msm::single(pts, nt, sc, cnt, c, res);
+    }
+    cl.l = msm::make_layout(cl.batch[0]);
     cl.total = off + cl.l.total;
     return cl;
 }
@@ -978,18 +990,56 @@ extern "C" cudaError_t msm(void *const *buffers, unsigned long *buffer_sizes, un
         char *base = reinterpret_cast<char *>(buffers[k]);
         CardLayout cl = card_layout(cnt, c, nt, base);
         u32 *d_points = reinterpret_cast<u32 *>(base + cl.points);
-        u32 *d_scalars = reinterpret_cast<u32 *>(base + cl.scalars);
         u32 *d_result = reinterpret_cast<u32 *>(base + cl.result);
-        cudaStream_t st = cudaStreamPerThread;
+        // Copies run on their own stream in the order scalars 0, points, scalars 1, 2, ...; the
+        // compute stream sorts batch 0's digits while the points arrive, and batch b + 1's
+        // scalars arrive while batch b is accumulated.
+        cudaStream_t st = cudaStreamPerThread, cs = nullptr;
+        cudaEvent_t pts_ready = nullptr, copied[2] = {nullptr, nullptr}, read[2] = {nullptr, nullptr};
+        err = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+        if (err == cudaSuccess) err = cudaEventCreateWithFlags(&pts_ready, cudaEventDisableTiming);
+        for (int i = 0; i < 2 && err == cudaSuccess; i++) {
+            err = cudaEventCreateWithFlags(&copied[i], cudaEventDisableTiming);
+            if (err == cudaSuccess) err = cudaEventCreateWithFlags(&read[i], cudaEventDisableTiming);
+        }
+        // the copy stream starts after any work the caller queued on the compute stream
+        if (err == cudaSuccess) err = cudaEventRecord(read[0], st);
+        if (err == cudaSuccess) err = cudaStreamWaitEvent(cs, read[0], 0);
+        auto copy_scalars = [&](u32 b) {
+            const int i = b & 1;
+            cudaError_t e = cudaSuccess;
+            if (b >= 2) e = cudaStreamWaitEvent(cs, read[i], 0);  // batch b - 2 is done with the buffer
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(base + cl.scalars[i], h_scaler_batch[b] + lo * 8, cnt * 32,
+                                    cudaMemcpyHostToDevice, cs);
+            if (e == cudaSuccess) e = cudaEventRecord(copied[i], cs);
+            return e;
+        };
+        if (batches > 0 && err == cudaSuccess) err = copy_scalars(0);
         for (u32 j = 0; j < nt && err == cudaSuccess; j++)
-            err = cudaMemcpyAsync(d_points + j * cnt * 16, h_points[j] + lo * 16, cnt * 64, cudaMemcpyHostToDevice, st);
+            err = cudaMemcpyAsync(d_points + j * cnt * 16, h_points[j] + lo * 16, cnt * 64, cudaMemcpyHostToDevice, cs);
+        if (err == cudaSuccess) err = cudaEventRecord(pts_ready, cs);
+        for (u32 b = 1; b < batches && b < 2 && err == cudaSuccess; b++) err = copy_scalars(b);
         for (u32 b = 0; b < batches && err == cudaSuccess; b++) {
-            err = cudaMemcpyAsync(d_scalars, h_scaler_batch[b] + lo * 8, cnt * 32, cudaMemcpyHostToDevice, st);
-            if (err == cudaSuccess) err = msm::run_batch(cl.batch, cl.l, base + cl.ws, st);
+            const int i = b & 1;
+            err = cudaStreamWaitEvent(st, copied[i], 0);
+            if (err == cudaSuccess)
+                err = msm::run_batch(cl.batch[i], cl.l, base + cl.ws, st, b == 0 ? pts_ready : nullptr, read[i]);
             if (err == cudaSuccess)
                 err = cudaMemcpyAsync(partial[k].data() + b * 16, d_result, 64, cudaMemcpyDeviceToHost, st);
+            if (err == cudaSuccess && b + 2 < batches) err = copy_scalars(b + 2);
         }
+        if (batches == 0 && err == cudaSuccess) err = cudaStreamWaitEvent(st, pts_ready, 0);
         if (err == cudaSuccess) err = cudaStreamSynchronize(st);
+        if (cs) {
+            cudaStreamSynchronize(cs);
+            cudaStreamDestroy(cs);
+        }
+        if (pts_ready) cudaEventDestroy(pts_ready);
+        for (int i = 0; i < 2; i++) {
+            if (copied[i]) cudaEventDestroy(copied[i]);
+            if (read[i]) cudaEventDestroy(read[i]);
+        }
     }
     // add the other cards' affine partials on the first card (msm_impl.cuh:902-907 does this
     // on the host; here it is one device addition per card)
