@@ -66,7 +66,7 @@ def test_fills(zk, orc):
     assert not t.numpy_u64().any()
 
 
-@pytest.mark.parametrize("n", [1, 5, 64, 65, 4097, 1 << 20])
+@pytest.mark.parametrize("n", [1, 5, 64, 65, 512, 513, 4097, 32769, 1 << 20])
 def test_poly_eval(zk, orc, n):
     a = orc.gen_fr(6, n)
     x = orc.gen_fr(7, 1)[0]
@@ -75,7 +75,7 @@ def test_poly_eval(zk, orc, n):
     assert np.array_equal(res.cpu().numpy().view(np.uint64)[0], orc.eval_poly(a, x))
 
 
-@pytest.mark.parametrize("n", [1, 63, 64, 65, 5000, 1 << 20])
+@pytest.mark.parametrize("n", [1, 63, 64, 65, 512, 513, 5000, 32769, 1 << 20])
 def test_batched_invert(zk, orc, n):
     a = orc.gen_fr(8, n)
     if n > 10:
@@ -87,7 +87,7 @@ def test_batched_invert(zk, orc, n):
     assert np.array_equal(t.numpy_u64(), orc.batch_invert(a))
 
 
-@pytest.mark.parametrize("n", [1, 64, 65, 4100, 70000])
+@pytest.mark.parametrize("n", [1, 64, 65, 512, 513, 4100, 32769, 70000])
 def test_scan_mul(zk, orc, n):
     a = orc.gen_fr(9, n)
     t = dev(zk, a)
@@ -100,7 +100,7 @@ def test_scan_mul(zk, orc, n):
     assert got == expect
 
 
-@pytest.mark.parametrize("log_n", [0, 1, 4, 6, 7, 12, 16])
+@pytest.mark.parametrize("log_n", [0, 1, 4, 6, 7, 9, 10, 12, 15, 16])
 def test_kate_division(zk, orc, log_n):
     n = 1 << log_n
     p = orc.gen_fr(10, n)

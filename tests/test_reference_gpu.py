@@ -218,10 +218,22 @@ def _temp_for(fn, *args):
     return torch.empty(max(size.value, 1), dtype=torch.uint8, device="cuda"), size
 
 
-@pytest.mark.parametrize("log_n", [10, 20])
+def _event_ms(fn, reps=5):
+    fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+@pytest.mark.parametrize("log_n", [10, 20, 22])
 def test_reference_poly_library_matches(zk, log_n):
     """poly_eval, batched_invert (with zeros), kate_division and scan_mul against the reference's
-    own kernels on the same inputs."""
+    own kernels on the same inputs; timed side by side at 2^22 with ZKP_REF_TIMING=1."""
     ref = _ref_poly(zk)
     n = 1 << log_n
     st = torch.cuda.current_stream().cuda_stream
@@ -259,3 +271,24 @@ def test_reference_poly_library_matches(zk, log_n):
     zk.poly.scan_mul(s_)
     torch.cuda.synchronize()
     assert torch.equal(s_ref.values, s_.values)
+    if TIMING and log_n == 22:
+        t_eval, z_eval = _temp_for(ref.poly_eval, p.poly_ptr(), None, None, None)
+        t_inv, z_inv = _temp_for(ref.batched_invert, a_ref.poly_ptr(), None)
+        t_kate, z_kate = _temp_for(ref.kate_division, log_n, p.poly_ptr(), None, q_ref.poly_ptr(), None)
+        t_scan, z_scan = _temp_for(ref.scan_mul, s_ref.poly_ptr(), None)
+        cases = [
+            ("poly_eval", lambda: ref.poly_eval(t_eval.data_ptr(), ctypes.byref(z_eval), p.poly_ptr(),
+                                                res_ref.data_ptr(), x.data_ptr(), st),
+             lambda: zk.poly.poly_eval(p, x, res)),
+            ("batched_invert", lambda: ref.batched_invert(t_inv.data_ptr(), ctypes.byref(z_inv), a_ref.poly_ptr(), st),
+             lambda: zk.poly.batched_invert(a)),
+            ("kate_division", lambda: ref.kate_division(t_kate.data_ptr(), ctypes.byref(z_kate), log_n, p.poly_ptr(),
+                                                        x.data_ptr(), q_ref.poly_ptr(), st),
+             lambda: zk.poly.kate_division(p, x, q)),
+            ("scan_mul", lambda: ref.scan_mul(t_scan.data_ptr(), ctypes.byref(z_scan), s_ref.poly_ptr(), st),
+             lambda: zk.poly.scan_mul(s_)),
+        ]
+        for name, run_ref, run in cases:
+            ms_ref, ms = _event_ms(run_ref), _event_ms(run)
+            print(json.dumps({"compare": name, "log_n": log_n, "reference_ms": ms_ref, "this_ms": ms,
+                              "speedup": ms_ref / ms}))

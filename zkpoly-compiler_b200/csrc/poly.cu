@@ -21,8 +21,15 @@
 namespace zk {
 namespace poly {
 
-constexpr u32 CHUNK = 64;   // elements folded by one thread
+constexpr u32 CHUNK = 64;   // elements folded by one thread on the first level
+constexpr u32 UPPER = 8;    // on the upper levels: short chains, since those levels are tiny
 constexpr u32 BLOCK = 128;
+
+// The level sweeps (evaluation, product scans, inversion, division) fold chunks of CHUNK
+// elements on the input and chunks of UPPER on every level above it: the first level carries
+// the work and wants long chains, the upper levels are a few thousand values whose cost is the
+// length of their dependent chains.
+inline u32 chunk_at(size_t level) { return level == 0 ? CHUNK : UPPER; }
 
 inline u32 grid_for(u64 items, u32 block, u32 per_sm = 16) {
     const u64 b = (items + block - 1) / block;
@@ -107,7 +114,7 @@ __global__ void __launch_bounds__(BLOCK) eval_level_kernel(View in, u64 n, const
     r.canonical().store(out + t * 8);
 }
 
-// powers for every level: X_0 = x, X_{k+1} = X_k^64, and X_k^16
+// powers for every level: X_0 = x, X_1 = X_0^CHUNK, X_{k+1} = X_k^UPPER, and X_k^16
 __global__ void eval_powers_kernel(const u32 *x, u32 levels, u32 *powers) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     Fr X = Fr::load(x);
@@ -116,19 +123,35 @@ __global__ void eval_powers_kernel(const u32 *x, u32 levels, u32 *powers) {
         for (int s = 0; s < 4; s++) x16 = Fr::sqr(x16);
         X.canonical().store(powers + (2 * k) * 8);
         x16.canonical().store(powers + (2 * k + 1) * 8);
-        Fr x64 = Fr::sqr(Fr::sqr(x16));
-        X = x64;
+        if (k == 0) {
+            X = Fr::sqr(Fr::sqr(x16));  // X^64
+        } else {
+            for (u32 s = 1; s < UPPER; s <<= 1) X = Fr::sqr(X);  // X^UPPER
+        }
     }
+}
+
+// an upper level: out[t] = sum_{i in chunk t} a_i X^(i - t*chunk), one Horner chain
+__global__ void __launch_bounds__(BLOCK) eval_small_kernel(View in, u64 n, const u32 *powers, u32 chunk, u32 *out) {
+    const u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    const u64 start = t * chunk;
+    if (start >= n) return;
+    const u64 end = start + chunk < n ? start + chunk : n;
+    const Fr X = Fr::load(powers);
+    Fr h = Fr::zero();
+    for (u64 i = end; i-- > start;) h = Fr::add(Fr::mul(h, X), Fr::load(in.at(i)));
+    h.canonical().store(out + t * 8);
 }
 
 // ------------------------------------------------------------------ chunked product sweeps
 // up-sweep: prefix[i] = running product (inclusive) within the chunk, zeros skipped when
 // skip_zero; tot[t] = chunk product
-__global__ void __launch_bounds__(BLOCK) prod_up_kernel(View in, u64 n, u32 *prefix, u32 *tot, bool skip_zero) {
+__global__ void __launch_bounds__(BLOCK) prod_up_kernel(View in, u64 n, u32 *prefix, u32 *tot, bool skip_zero,
+                                                      u32 chunk) {
     const u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x;
-    const u64 start = t * CHUNK;
+    const u64 start = t * chunk;
     if (start >= n) return;
-    const u64 end = start + CHUNK < n ? start + CHUNK : n;
+    const u64 end = start + chunk < n ? start + chunk : n;
     Fr acc = Fr::one();
     for (u64 i = start; i < end; i++) {
         Fr a = Fr::load(in.at(i));
@@ -139,11 +162,12 @@ __global__ void __launch_bounds__(BLOCK) prod_up_kernel(View in, u64 n, u32 *pre
 }
 
 // batched inversion down-sweep: inv_tot[t] = (chunk product)^-1; walks the chunk backwards
-__global__ void __launch_bounds__(BLOCK) inv_down_kernel(View data, u64 n, const u32 *prefix, const u32 *inv_tot) {
+__global__ void __launch_bounds__(BLOCK) inv_down_kernel(View data, u64 n, const u32 *prefix, const u32 *inv_tot,
+                                                       u32 chunk) {
     const u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x;
-    const u64 start = t * CHUNK;
+    const u64 start = t * chunk;
     if (start >= n) return;
-    const u64 end = start + CHUNK < n ? start + CHUNK : n;
+    const u64 end = start + chunk < n ? start + chunk : n;
     Fr inv = Fr::load(inv_tot + t * 8);
     for (u64 i = end; i-- > start;) {
         u32 *p = data.at(i);
@@ -158,11 +182,11 @@ __global__ void __launch_bounds__(BLOCK) inv_down_kernel(View data, u64 n, const
 
 // inclusive product scan down-sweep: `above` is the inclusive scan of the chunk products (or
 // null for the top level), so chunk t starts from above[t-1] (1 for t = 0)
-__global__ void __launch_bounds__(BLOCK) scan_down_kernel(View data, u64 n, const u32 *above) {
+__global__ void __launch_bounds__(BLOCK) scan_down_kernel(View data, u64 n, const u32 *above, u32 chunk) {
     const u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x;
-    const u64 start = t * CHUNK;
+    const u64 start = t * chunk;
     if (start >= n) return;
-    const u64 end = start + CHUNK < n ? start + CHUNK : n;
+    const u64 end = start + chunk < n ? start + chunk : n;
     Fr acc = (above && t > 0) ? Fr::load(above + (t - 1) * 8) : Fr::one();
     for (u64 i = start; i < end; i++) {
         u32 *p = data.at(i);
@@ -206,11 +230,11 @@ __global__ void scan_top_kernel(u32 *vals, u64 m) {
 // with zero carry-in; a chunk's carry is q at its first index.  Up-sweep: local value at the
 // chunk start (Horner over the chunk from its top); the carries combine as another reversed
 // Horner with base b^CHUNK; down-sweep walks each chunk downwards from its carry-in.
-__global__ void __launch_bounds__(BLOCK) kate_up_kernel(View p, u64 n, const u32 *b, u32 *loc) {
+__global__ void __launch_bounds__(BLOCK) kate_up_kernel(View p, u64 n, const u32 *b, u32 *loc, u32 chunk) {
     const u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x;
-    const u64 start = t * CHUNK;
+    const u64 start = t * chunk;
     if (start >= n) return;
-    const u64 end = start + CHUNK < n ? start + CHUNK : n;
+    const u64 end = start + chunk < n ? start + chunk : n;
     const Fr B = Fr::load(b);
     // value of q at `start` from the chunk's own terms: sum_{start < j < end+... }
     Fr acc = Fr::zero();
@@ -223,10 +247,10 @@ __global__ void __launch_bounds__(BLOCK) kate_up_kernel(View p, u64 n, const u32
     acc.canonical().store(loc + t * 8);
 }
 
-// base of the next level: B^CHUNK
-__global__ void pow_chunk_kernel(const u32 *b, u32 *out) {
+// base of the next level: B^chunk
+__global__ void pow_chunk_kernel(const u32 *b, u32 chunk, u32 *out) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    Fr::pow_u64(Fr::load(b), CHUNK).canonical().store(out);
+    Fr::pow_u64(Fr::load(b), chunk).canonical().store(out);
 }
 
 // a short level (n <= CHUNK): one thread runs the recurrence directly
@@ -242,11 +266,12 @@ __global__ void kate_small_kernel(View p, View q, u64 n, const u32 *b) {
     }
 }
 
-__global__ void __launch_bounds__(BLOCK) kate_down_kernel(View p, View q, u64 n, const u32 *b, const u32 *carry) {
+__global__ void __launch_bounds__(BLOCK) kate_down_kernel(View p, View q, u64 n, const u32 *b, const u32 *carry,
+                                                        u32 chunk) {
     const u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x;
-    const u64 start = t * CHUNK;
+    const u64 start = t * chunk;
     if (start >= n) return;
-    const u64 end = start + CHUNK < n ? start + CHUNK : n;
+    const u64 end = start + chunk < n ? start + chunk : n;
     const Fr B = Fr::load(b);
     // carry[t] = q at the first index of chunk t + 1: with loc the chunk-local values, that is
     // the next level's quotient at t (which is 0 for the last chunk)
@@ -263,11 +288,11 @@ __global__ void __launch_bounds__(BLOCK) kate_down_kernel(View p, View q, u64 n,
 inline std::vector<u64> level_sizes(u64 n) {
     std::vector<u64> s;
     u64 m = n;
-    while (m > CHUNK) {
-        m = (m + CHUNK - 1) / CHUNK;
+    for (size_t k = 0; m > chunk_at(k); k++) {
+        m = (m + chunk_at(k) - 1) / chunk_at(k);
         s.push_back(m);
     }
-    return s;  // sizes of the chunk-result arrays, last one <= CHUNK
+    return s;  // sizes of the chunk-result arrays; the last one fits in one chunk of its level
 }
 
 inline size_t al(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -354,8 +379,13 @@ extern "C" cudaError_t poly_eval(void *temp_buf, unsigned long *temp_buf_size, C
     u64 m = n;
     for (u32 k = 0; k < levels; k++) {
         u32 *out = (k + 1 < levels) ? reinterpret_cast<u32 *>(base + off) : res;
-        const u64 threads = (m + CHUNK - 1) / CHUNK;
-        eval_level_kernel<<<(u32)((threads + BLOCK - 1) / BLOCK), BLOCK, 0, stream>>>(in, m, powers + 2 * k * 8, out);
+        const u32 chunk = chunk_at(k);
+        const u64 threads = (m + chunk - 1) / chunk;
+        const u32 grid = (u32)((threads + BLOCK - 1) / BLOCK);
+        if (k == 0)
+            eval_level_kernel<<<grid, BLOCK, 0, stream>>>(in, m, powers, out);
+        else
+            eval_small_kernel<<<grid, BLOCK, 0, stream>>>(in, m, powers + 2 * k * 8, chunk, out);
         ZK_TRY(cudaGetLastError());
         if (k + 1 < levels) {
             in = plain_view(out, threads);
@@ -404,18 +434,20 @@ extern "C" cudaError_t batched_invert(void *temp_buffer, unsigned long *buffer_s
     const size_t L = data.size();
     for (size_t k = 0; k < L; k++) {
         const u64 m = size[k];
-        const u64 threads = (m + CHUNK - 1) / CHUNK;
+        const u64 threads = (m + chunk_at(k) - 1) / chunk_at(k);
         u32 *tot = (k + 1 < L) ? data[k + 1].base : top;
-        prod_up_kernel<<<(u32)((threads + BLOCK - 1) / BLOCK), BLOCK, 0, stream>>>(data[k], m, prefix[k], tot, k == 0);
+        prod_up_kernel<<<(u32)((threads + BLOCK - 1) / BLOCK), BLOCK, 0, stream>>>(data[k], m, prefix[k], tot, k == 0,
+                                                                                  chunk_at(k));
         ZK_TRY(cudaGetLastError());
     }
     inv_top_kernel<<<1, 32, 0, stream>>>(top, 1);
     ZK_TRY(cudaGetLastError());
     for (size_t k = L; k-- > 0;) {
         const u64 m = size[k];
-        const u64 threads = (m + CHUNK - 1) / CHUNK;
+        const u64 threads = (m + chunk_at(k) - 1) / chunk_at(k);
         const u32 *inv_tot = (k + 1 < L) ? data[k + 1].base : top;
-        inv_down_kernel<<<(u32)((threads + BLOCK - 1) / BLOCK), BLOCK, 0, stream>>>(data[k], m, prefix[k], inv_tot);
+        inv_down_kernel<<<(u32)((threads + BLOCK - 1) / BLOCK), BLOCK, 0, stream>>>(data[k], m, prefix[k], inv_tot,
+                                                                                   chunk_at(k));
         ZK_TRY(cudaGetLastError());
     }
     return cudaSuccess;
@@ -446,15 +478,17 @@ extern "C" cudaError_t scan_mul(void *temp_buffer, unsigned long *buffer_size, P
     }
     const size_t L = data.size();
     for (size_t k = 0; k + 1 < L; k++) {
-        const u64 threads = (size[k] + CHUNK - 1) / CHUNK;
+        const u64 threads = (size[k] + chunk_at(k) - 1) / chunk_at(k);
         prod_up_kernel<<<(u32)((threads + BLOCK - 1) / BLOCK), BLOCK, 0, stream>>>(data[k], size[k], nullptr,
-                                                                                  data[k + 1].base, false);
+                                                                                  data[k + 1].base, false,
+                                                                                  chunk_at(k));
         ZK_TRY(cudaGetLastError());
     }
     for (size_t k = L; k-- > 0;) {
-        const u64 threads = (size[k] + CHUNK - 1) / CHUNK;
+        const u64 threads = (size[k] + chunk_at(k) - 1) / chunk_at(k);
         const u32 *above = (k + 1 < L) ? data[k + 1].base : nullptr;
-        scan_down_kernel<<<(u32)((threads + BLOCK - 1) / BLOCK), BLOCK, 0, stream>>>(data[k], size[k], above);
+        scan_down_kernel<<<(u32)((threads + BLOCK - 1) / BLOCK), BLOCK, 0, stream>>>(data[k], size[k], above,
+                                                                                    chunk_at(k));
         ZK_TRY(cudaGetLastError());
     }
     return cudaSuccess;
@@ -491,22 +525,22 @@ extern "C" cudaError_t kate_division(void *temp_buf, unsigned long *temp_buf_siz
         Q.push_back(plain_view(base + off, lv[k]));
         off += al(lv[k] * 32);
         size.push_back(lv[k]);
-        pow_chunk_kernel<<<1, 32, 0, stream>>>(Bs.back(), bases + k * 8);
+        pow_chunk_kernel<<<1, 32, 0, stream>>>(Bs.back(), chunk_at(k), bases + k * 8);
         Bs.push_back(bases + k * 8);
     }
     // up-sweeps: P[k+1][t] = chunk-local value of level k at chunk t's start
     for (size_t k = 0; k + 1 < L; k++) {
-        const u64 chunks = (size[k] + CHUNK - 1) / CHUNK;
+        const u64 chunks = (size[k] + chunk_at(k) - 1) / chunk_at(k);
         kate_up_kernel<<<(u32)((chunks + BLOCK - 1) / BLOCK), BLOCK, 0, stream>>>(P[k], size[k], Bs[k],
-                                                                                 P[k + 1].base);
+                                                                                 P[k + 1].base, chunk_at(k));
         ZK_TRY(cudaGetLastError());
     }
     kate_small_kernel<<<1, 32, 0, stream>>>(P[L - 1], Q[L - 1], size[L - 1], Bs[L - 1]);
     ZK_TRY(cudaGetLastError());
     for (size_t k = L - 1; k-- > 0;) {
-        const u64 chunks = (size[k] + CHUNK - 1) / CHUNK;
+        const u64 chunks = (size[k] + chunk_at(k) - 1) / chunk_at(k);
         kate_down_kernel<<<(u32)((chunks + BLOCK - 1) / BLOCK), BLOCK, 0, stream>>>(P[k], Q[k], size[k], Bs[k],
-                                                                                   Q[k + 1].base);
+                                                                                   Q[k + 1].base, chunk_at(k));
         ZK_TRY(cudaGetLastError());
     }
     return cudaSuccess;
