@@ -48,6 +48,16 @@ unsigned long long zkp_msm_workspace_size(unsigned long long n, unsigned int win
 /* Window width the library picks for n points when window == 0. */
 unsigned int zkp_msm_default_window(unsigned long long n);
 
+/* Affine pairing rounds for MSMs planned after this call (-1 = chosen by size, the default;
+ * else 0..4).  Each round halves every bucket's point list with affine additions whose
+ * inverses share one inversion (Montgomery's trick) before the XYZZ bucket walk.  The
+ * workspace size depends on it: query sizes and run under the same setting. */
+cudaError_t zkp_msm_set_affine_rounds(int rounds);
+
+/* The number of pairing rounds an MSM of n points (window, n_tables as for
+ * zkp_msm_workspace_size) runs under the current setting. */
+unsigned int zkp_msm_rounds_for(unsigned long long n, unsigned int window, unsigned int n_tables);
+
 /* result_d (64-byte affine) = sum_i scalars_d[i] * points_d[i], asynchronous on `stream`.
  * points_d holds n_tables contiguous tables of n affine points (table j = 2^(j*Wp*window) P
  * with Wp = ceil(ceil(254/window) / n_tables)); workspace_d is caller-owned, at least

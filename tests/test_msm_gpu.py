@@ -140,3 +140,77 @@ def test_msm_batch_uneven(zk, orc):
     torch.cuda.synchronize()
     for t, e in zip(tasks, expect):
         assert np.array_equal(t["result"].cpu().numpy().view(np.uint64), e)
+
+
+def _device_msm(zk, s, p, window, n_tables=1):
+    n = s.shape[0]
+    bases = zk.msm.ResidentBases(p, window=window, n_tables=n_tables)
+    res = torch.zeros(16, dtype=torch.int32, device="cuda")
+    dev_s = torch.from_numpy(s.view(np.int32).reshape(n, 8).copy()).cuda()
+    bases.msm(dev_s, res, bases.workspace())
+    return res.cpu().numpy().view(np.uint64)
+
+
+@pytest.mark.parametrize("rounds", [0, 1, 2, 3, 4])
+def test_msm_affine_rounds(zk, orc, rounds):
+    """A fixed number of affine pairing rounds on buckets that hold equal points (doubling
+    pairs), opposite points (pairs summing to the identity), identity bases and zero scalars."""
+    n = 4096
+    s = orc.gen_fr(500, n)
+    p = orc.gen_points(501, n)
+    s[0:300] = s[300]                              # one digit per window for 301 records
+    p[0:200] = p[300]                              # equal points in one bucket
+    p[200:300] = p[300]
+    p[200:300, 4:8] = orc.neg(p[300, 4:8], orc.FQ)  # and their negatives
+    p[400:440] = 0                                 # identity bases
+    s[440:500] = 0                                 # zero scalars
+    expect = orc.best_multiexp(s, p)
+    zk.msm.set_affine_rounds(rounds)
+    try:
+        for window, n_tables in ((8, 1), (13, 1), (11, 24)):
+            assert np.array_equal(_device_msm(zk, s, p, window, n_tables), expect), (window, n_tables)
+    finally:
+        zk.msm.set_affine_rounds(-1)
+
+
+@pytest.mark.parametrize("rounds", [2, 4])
+def test_msm_affine_rounds_degenerate(zk, orc, rounds):
+    """Every record of a window in one bucket: all doublings, then P + (-P) cancellations."""
+    n = 1 << 12
+    P = orc.gen_points(502, 1)[0]
+    s = np.repeat(orc.gen_fr(503, 1), n, axis=0)
+    p = np.repeat(P[None, :], n, axis=0)
+    zk.msm.set_affine_rounds(rounds)
+    try:
+        assert np.array_equal(_device_msm(zk, s, p, 10), orc.best_multiexp(s, p))
+        p[1::3, 4:8] = orc.neg(P[4:8], orc.FQ)        # a third of them negated
+        assert np.array_equal(_device_msm(zk, s, p, 10), orc.best_multiexp(s, p))
+        p[::2, 4:8] = orc.neg(P[4:8], orc.FQ)
+        p[1::2] = P                                    # alternate P, -P: the sum is the identity
+        assert np.array_equal(_device_msm(zk, s, p, 10), np.zeros(8, dtype=np.uint64))
+    finally:
+        zk.msm.set_affine_rounds(-1)
+
+
+def test_msm_batch_affine_rounds(zk, orc):
+    """The batched form with pairing rounds: tasks of different sizes and windows share the
+    rounds' lists (bucket ids are global across tasks)."""
+    sizes, windows = [3000, 1, 20000, 777, 5000], [8, 0, 16, 11, 20]
+    N = max(sizes)
+    base_pts = orc.gen_points(510, N)
+    pts_dev = torch.from_numpy(base_pts.view(np.int32).reshape(N, 16).copy()).cuda()
+    zk.msm.set_affine_rounds(3)
+    try:
+        tasks, expect = [], []
+        for i, (n, w) in enumerate(zip(sizes, windows)):
+            s = orc.gen_fr(520 + i, n)
+            tasks.append({"points": pts_dev, "n": n, "window": w,
+                          "scalars": torch.from_numpy(s.view(np.int32).reshape(-1, 8).copy()).cuda(),
+                          "result": torch.zeros(16, dtype=torch.int32, device="cuda")})
+            expect.append(orc.best_multiexp(s, base_pts[:n]))
+        batch = zk.msm.MsmBatch(tasks)
+        batch.run()
+        for t, e in zip(tasks, expect):
+            assert np.array_equal(t["result"].cpu().numpy().view(np.uint64), e)
+    finally:
+        zk.msm.set_affine_rounds(-1)

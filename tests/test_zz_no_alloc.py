@@ -45,6 +45,16 @@ def test_noalloc_matches_workspace_entry_two_calls(zk):
 
 
 def test_noalloc_largest_fitting_size_and_refusal(zk):
+    # the fixed array holds the layout without affine pairing rounds (the entry never runs
+    # them), so the size queries below are made under that setting
+    zk.msm.set_affine_rounds(0)
+    try:
+        _largest_fitting_size_and_refusal(zk)
+    finally:
+        zk.msm.set_affine_rounds(-1)
+
+
+def _largest_fitting_size_and_refusal(zk):
     lib = zk.native.load("libmsm.so")
     cap = lib.zkp_msm_noalloc_capacity()
     assert cap == 64 << 20

@@ -72,6 +72,7 @@ struct Batch {
     u64 seg_first[MAX_TASKS + 1];  // reduction segments (key count / L)
     u32 win_first[MAX_TASKS + 1];  // physical windows
     u32 ncls, nparts;              // largest class count / parts of any task (reduction grid)
+    u32 rounds;                    // affine pairing rounds before the XYZZ walk (0 = none)
 };
 
 template <typename T>
@@ -117,8 +118,25 @@ inline u32 default_window(u64 n) {
     return best;
 }
 
-// fills the prefixes and the chunk size; tasks[] must be set
-inline void finish_batch(Batch &b) {
+// Affine pairing rounds (stage 4a below): -1 chooses by size, else a fixed count.
+constexpr u32 MAX_ROUNDS = 4;
+constexpr u32 KA = 64;  // list elements per thread in a pairing round (at most KA / 2 pairs)
+inline int &affine_rounds_setting() {
+    static int r = -1;
+    return r;
+}
+inline u32 auto_rounds(u64 entries) { return entries >= (1ull << 24) ? 3u : 0u; }
+
+// upper bounds of the list lengths: E_0 = live digits, E_{r+1} <= sum_b (m_b / 2 + 1) =
+// E_r / 2 + nb (a bucket's run leaves at most one unpaired point at each end)
+inline u64 next_list_bound(u64 e, u64 nb) {
+    const u64 x = (e + 1) / 2 + nb;
+    return x < e ? x : e;
+}
+
+// fills the prefixes and the chunk size; tasks[] must be set.  rounds < 0: the library
+// setting (itself -1 = by size).
+inline void finish_batch(Batch &b, int rounds = -1) {
     b.sc_first[0] = b.key_first[0] = b.seg_first[0] = 0;
     b.win_first[0] = 0;
     b.ncls = b.nparts = 1;
@@ -133,7 +151,12 @@ inline void finish_batch(Batch &b) {
         b.nparts = b.nparts > k.parts ? b.nparts : k.parts;
         entries += k.n * k.W;
     }
-    // chunk so that roughly 4 waves of 384 threads per SM cover the entries
+    if (rounds < 0) rounds = affine_rounds_setting();
+    b.rounds = rounds < 0 ? auto_rounds(entries) : (u32)(rounds > (int)MAX_ROUNDS ? MAX_ROUNDS : rounds);
+    u64 walk = entries;
+    for (u32 r = 0; r < b.rounds; r++) walk = next_list_bound(walk, b.key_first[b.ntasks]);
+    entries = walk;
+    // chunk so that roughly 4 waves of 384 threads per SM cover the walk's entries
     const u64 threads = (u64)num_sms() * 384 * 4;
     u64 k = (entries + threads - 1) / threads;
     if (k < 8) k = 8;
@@ -142,13 +165,28 @@ inline void finish_batch(Batch &b) {
 }
 
 // ------------------------------------------------------------------ workspace layout
+// Montgomery-trick tree over a round's thread totals: a CTA of TREE_CTA threads folds
+// TREE_CTA * TREE_PER values per level, so two levels and the top cover 2^36 values
+constexpr u32 TREE_CTA = 256, TREE_PER = 16;
+constexpr u64 TREE_SPAN = (u64)TREE_CTA * TREE_PER;
+constexpr u32 TREE_LEVELS = 3;
+
 struct Layout {
     size_t counts, cursor, sorted_bucket, sorted_point, bucket_sums, part_pts, part_bucket, part_flag, long_list,
-        seg, cls, win, total;
+        seg, cls, win, scan_sums, total;
     u64 nb, entries, chunks, segs, wins;
+    // affine pairing rounds: list r + 1 (r < rounds) lives in buffer r % 2; starts[r] are the
+    // bucket starts of list r (starts[0] = the counts region); thr[r] threads in round r
+    u32 rounds;
+    u64 emax[MAX_ROUNDS + 1], thr[MAX_ROUNDS];
+    size_t starts[MAX_ROUNDS + 1], lst_bkt[2], lst_pts[2], prefix[MAX_ROUNDS], tvals;
+    // per tree level: member prefixes, per-thread exclusive prefix / suffix products, and the
+    // next level's values (the CTA products)
+    size_t tree_pre[TREE_LEVELS + 1], tree_ex[TREE_LEVELS + 1], tree_sx[TREE_LEVELS + 1], tree_dat[TREE_LEVELS + 1];
 };
 
 inline size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
+
 
 inline Layout make_layout(const Batch &b) {
     Layout l{};
@@ -161,13 +199,51 @@ inline Layout make_layout(const Batch &b) {
     l.nb = b.key_first[b.ntasks];
     l.entries = 0;
     for (u32 t = 0; t < b.ntasks; t++) l.entries += b.task[t].n * b.task[t].W;
-    l.chunks = (l.entries + b.K - 1) / b.K;
     l.segs = b.seg_first[b.ntasks];
     l.wins = b.win_first[b.ntasks];
+    l.rounds = b.rounds;
+    l.emax[0] = l.entries;
+    for (u32 r = 0; r < l.rounds; r++) {
+        l.emax[r + 1] = next_list_bound(l.emax[r], l.nb);
+        l.thr[r] = (l.emax[r] + KA - 1) / KA;
+    }
+    l.chunks = (l.emax[l.rounds] + b.K - 1) / b.K;
     l.counts = take((l.nb + 1) * 4);
     l.cursor = take((l.nb + 1) * 4);
+    l.scan_sums = take(((l.nb + 1) / 4096 + 2) * 4);
     l.sorted_bucket = take(l.entries * 4);
     l.sorted_point = take(l.entries * 4);
+    if (l.rounds) {
+        l.starts[0] = l.counts;
+        for (u32 r = 1; r <= l.rounds; r++) l.starts[r] = take((l.nb + 1) * 4);
+        for (u32 i = 0; i < 2 && i < l.rounds; i++) {
+            l.lst_bkt[i] = take(l.emax[i + 1] * 4);
+            l.lst_pts[i] = take(l.emax[i + 1] * 64);
+        }
+        // Prefix products (slot-major, KA / 2 slots a thread).  Round 0 keeps them in list
+        // buffer 1, which round 1 fills only later; the later rounds in the sorted arrays,
+        // which round 0 has consumed.  Either falls back to space of its own when too small.
+        const u64 pre0 = l.thr[0] * (KA / 2) * 32;
+        l.prefix[0] = (l.rounds >= 2 && pre0 <= l.emax[2] * 64) ? l.lst_pts[1] : take(pre0);
+        if (l.rounds >= 2) {
+            const u64 pre1 = l.thr[1] * (KA / 2) * 32;  // thr[r] <= thr[1] for r >= 1
+            const size_t sorted_bytes = l.sorted_point + l.entries * 4 - l.sorted_bucket;
+            const size_t at1 = pre1 <= sorted_bytes ? l.sorted_bucket : take(pre1);
+            for (u32 r = 1; r < l.rounds; r++) l.prefix[r] = at1;
+        }
+        l.tvals = take(l.thr[0] * 32);
+        u64 m = l.thr[0];
+        for (u32 k = 0; k <= TREE_LEVELS; k++) l.tree_pre[k] = l.tree_ex[k] = l.tree_sx[k] = l.tree_dat[k] = 0;
+        for (u32 k = 0; k <= TREE_LEVELS; k++) {
+            l.tree_pre[k] = take(m * 32);  // the top level uses only this one
+            if (m <= TREE_SPAN) break;
+            const u64 ctas = (m + TREE_SPAN - 1) / TREE_SPAN;
+            l.tree_ex[k] = take(ctas * TREE_CTA * 32);
+            l.tree_sx[k] = take(ctas * TREE_CTA * 32);
+            m = ctas;
+            l.tree_dat[k + 1] = take(m * 32);
+        }
+    }
     l.bucket_sums = take(l.nb * 128);
     l.part_pts = take(l.chunks * 2 * 128);
     l.part_bucket = take(l.chunks * 2 * 4);
@@ -179,6 +255,9 @@ inline Layout make_layout(const Batch &b) {
     l.total = off;
     return l;
 }
+
+// canonical negation: q - y, with 0 kept
+ZK_DI Fq neg_canonical(const Fq &y) { return Fq::sub_c(Fq::zero(), y); }
 
 // ------------------------------------------------------------------ 1 + 3: digits
 // signed c-bit digits of the canonical scalar, least significant window first
@@ -357,6 +436,9 @@ ZK_DI G1A fetch_point(const u32 *points, u32 code) {
 #ifndef ZK_ACC_MIN_BLOCKS
 #define ZK_ACC_MIN_BLOCKS 2  // resident CTAs of 256 threads per SM the register budget targets
 #endif
+// CODES: the walk reads list 0 (point codes into the task tables); otherwise the explicit
+// points of the last pairing round's list, at their list positions.
+template <bool CODES>
 __global__ void __launch_bounds__(256, ZK_ACC_MIN_BLOCKS) accumulate_kernel(const Batch b, const u32 *sorted_bucket,
                                                            const u32 *sorted_point, const u32 *live,
                                                            u32 *bucket_sums, u32 *part_pts, u32 *part_bucket,
@@ -369,8 +451,9 @@ __global__ void __launch_bounds__(256, ZK_ACC_MIN_BLOCKS) accumulate_kernel(cons
     const bool from_prev = start > 0 && sorted_bucket[start - 1] == sorted_bucket[start];
     u64 run_start = start;
     u32 cur = sorted_bucket[start];
-    const u32 *pts = b.task[find_task(b.key_first, b.ntasks, (u64)cur)].points;
-    G1X acc = G1X::from_affine(fetch_point(pts, sorted_point[start]));
+    const u32 *pts = CODES ? b.task[find_task(b.key_first, b.ntasks, (u64)cur)].points : sorted_point;
+    G1X acc = G1X::from_affine(CODES ? fetch_point(pts, sorted_point[start])
+                                     : G1A::load_nc(sorted_point + start * 16));
     // The next record's bucket, code and point address are read one iteration ahead; its point
     // is loaded when it is used.  (Keeping the point load itself one iteration ahead helped
     // while the Fq product was slower; with the paired product the 16 registers it holds cost
@@ -380,9 +463,13 @@ __global__ void __launch_bounds__(256, ZK_ACC_MIN_BLOCKS) accumulate_kernel(cons
     const u32 *naddr = pts;
     if (start + 1 < end) {
         nbk = sorted_bucket[start + 1];
-        ncode = sorted_point[start + 1];
-        if (nbk != cur) npts = b.task[find_task(b.key_first, b.ntasks, (u64)nbk)].points;
-        naddr = npts + (u64)(ncode & 0x7fffffffu) * 16;
+        if (CODES) {
+            ncode = sorted_point[start + 1];
+            if (nbk != cur) npts = b.task[find_task(b.key_first, b.ntasks, (u64)nbk)].points;
+            naddr = npts + (u64)(ncode & 0x7fffffffu) * 16;
+        } else {
+            naddr = sorted_point + (start + 1) * 16;
+        }
     }
     for (u64 p = start + 1; p <= end; p++) {
         const u32 bk = nbk, code = ncode;
@@ -391,13 +478,17 @@ __global__ void __launch_bounds__(256, ZK_ACC_MIN_BLOCKS) accumulate_kernel(cons
         if (p < end) pt = G1A::load_nc(naddr);
         if (p + 1 < end) {
             nbk = sorted_bucket[p + 1];
-            ncode = sorted_point[p + 1];
-            if (nbk != bk) npts = b.task[find_task(b.key_first, b.ntasks, (u64)nbk)].points;
-            naddr = npts + (u64)(ncode & 0x7fffffffu) * 16;
+            if (CODES) {
+                ncode = sorted_point[p + 1];
+                if (nbk != bk) npts = b.task[find_task(b.key_first, b.ntasks, (u64)nbk)].points;
+                naddr = npts + (u64)(ncode & 0x7fffffffu) * 16;
+            } else {
+                naddr = sorted_point + (p + 1) * 16;
+            }
         } else {
             nbk = EMPTY;
         }
-        if (p < end && (code & 0x80000000u)) pt = pt.neg();
+        if (CODES && p < end && (code & 0x80000000u)) pt = pt.neg();
         if (p < end && bk == cur) {
             acc = g1_madd(acc, pt);
             continue;
@@ -490,6 +581,251 @@ __global__ void __launch_bounds__(128) long_chain_kernel(const u32 *live, u32 K,
         if (threadIdx.x == 0) G1X::load(sm).store(bucket_sums + (u64)bucket * 32);
         __syncthreads();
     }
+}
+
+// ------------------------------------------------------------------ 4a: affine pairing rounds
+// Before the XYZZ walk, each round roughly halves every bucket's list: list positions 2k and
+// 2k + 1 (pair slot k) holding two points of the same bucket are added in affine coordinates;
+// a point whose slot partner belongs to another bucket (at most one at each end of a bucket's
+// run) is carried unchanged.  Round r reads list r and writes list r + 1, in which bucket b
+// starts at s'_b = sum_{b' < b} m'_b with m'_b = o + ceil((m_b - o) / 2), o = s_b mod 2, and
+// the point from position e of bucket b lands at s'_b + (e - s_b + o) / 2.  Slot-major
+// indexing (thread t takes slots t, t + T, t + 2T, ...) keeps every list access coalesced.
+//
+// An affine sum needs one inverse; a round shares one inversion among all its pairs by
+// Montgomery's trick: each thread chains the denominators of its pairs (KA / 2 slots), a
+// product tree over the thread totals ends in one inversion, and each thread then walks its
+// slots backwards, recovering every denominator's inverse with two products.  A pair costs six
+// products (three for the trick; the slope, its square, and the new y), against ten for the
+// mixed XYZZ addition it replaces.  The bucket sums, and so the result, are the same.
+
+// list r + 1's counts from list r's starts; entry nb is 0 (the scan's total)
+__global__ void halve_counts_kernel(const u32 *starts, u64 nb, u32 *cnt) {
+    const u64 b = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b > nb) return;
+    u32 m = 0;
+    if (b < nb) {
+        const u32 s0 = starts[b], mb = starts[b + 1] - s0, o = s0 & 1u;
+        m = mb == 0 ? 0u : o + ((mb - o + 1) >> 1);
+    }
+    cnt[b] = m;
+}
+
+
+// Address of the point at list position e, and its sign code.  CODES: list 0, whose entries
+// are point codes into the bucket's task tables (index | sign << 31); otherwise explicit
+// 64-byte canonical affine points.
+template <bool CODES>
+ZK_DI const u32 *list_addr(const Batch &b, const u32 *pts, u64 e, u32 bucket, u32 &code) {
+    if (CODES) {
+        code = pts[e];
+        const u32 *tbl = b.task[find_task(b.key_first, b.ntasks, (u64)bucket)].points;
+        return tbl + (u64)(code & 0x7fffffffu) * 16;
+    }
+    code = 0;
+    return pts + e * 16;
+}
+ZK_DI G1A signed_point(const u32 *addr, u32 code) {
+    G1A a = G1A::load_nc(addr);
+    if (code & 0x80000000u) a.y = neg_canonical(a.y);
+    return a;
+}
+
+// pair kinds: 0 general (d = x2 - x1), 1 doubling (d = 2 y1), 2 first is the identity (sum =
+// second), 3 second is the identity (sum = first), 4 opposite points (sum = identity); kinds
+// 2-4 use d = 1.  A point is the identity exactly when y == 0 (canonical); a valid point with
+// x != 0 is never the identity, so x1 != x2 with both non-zero decides kind 0 from x alone.
+ZK_DI bool general_by_x(const Fq &x1, const Fq &x2) { return !x1.is_zero() && !x2.is_zero() && !(x1 == x2); }
+ZK_DI u32 pair_kind(const G1A &a, const G1A &c) {
+    if (general_by_x(a.x, c.x)) return 0;
+    if (a.y.is_zero()) return 2;
+    if (c.y.is_zero()) return 3;
+    if (!(a.x == c.x)) return 0;
+    return a.y == c.y ? 1u : 4u;
+}
+ZK_DI Fq pair_den(const G1A &a, const G1A &c, u32 kind) {
+    if (kind == 0) return Fq::sub(c.x, a.x);
+    if (kind == 1) return Fq::dbl(a.y);
+    return Fq::one();
+}
+ZK_DI G1A pair_sum(const G1A &a, const G1A &c, u32 kind, const Fq &inv) {
+    if (kind == 2) return c;
+    if (kind == 3) return a;
+    G1A r;
+    if (kind == 4) {
+        r.x = Fq::zero();
+        r.y = Fq::zero();
+        return r;
+    }
+    Fq lam;
+    if (kind == 0) {
+        lam = fmul(Fq::sub(c.y, a.y), inv);
+    } else {
+        const Fq x2 = fsqr(a.x);
+        lam = fmul(Fq::add(Fq::dbl(x2), x2), inv);
+    }
+    const Fq x3 = Fq::sub(Fq::sub(fsqr(lam), a.x), c.x);
+    r.y = Fq::sub(fmul(lam, Fq::sub(a.x, x3)), a.y).canonical();
+    r.x = x3.canonical();
+    return r;
+}
+
+// Up pass: for each of the thread's pair slots that holds a pair, store the product of the
+// thread's earlier denominators (slot-major, prefix[k T + t]) and chain this one; tot[t] is
+// the product of all of them (1 when the thread has none).
+template <bool CODES>
+__global__ void __launch_bounds__(256) pair_up_kernel(const Batch b, const u32 *bkt, const u32 *pts,
+                                                     const u32 *starts, u64 nb, u64 nthr, u32 *prefix, u32 *tot) {
+    const u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nthr) return;
+    const u64 E = starts[nb];
+    Fq acc = Fq::one();
+    for (u32 k = 0; k < KA / 2; k++) {
+        const u64 e0 = 2 * (t + (u64)k * nthr);
+        if (e0 + 1 >= E) break;
+        const u32 b0 = bkt[e0];
+        if (bkt[e0 + 1] != b0) continue;
+        u32 c0, c1;
+        const u32 *a0 = list_addr<CODES>(b, pts, e0, b0, c0);
+        const u32 *a1 = list_addr<CODES>(b, pts, e0 + 1, b0, c1);
+        const Fq x1 = Fq::load_nc(a0), x2 = Fq::load_nc(a1);
+        Fq d;
+        if (general_by_x(x1, x2)) {
+            d = Fq::sub(x2, x1);
+        } else {
+            const G1A pa = signed_point(a0, c0), pc = signed_point(a1, c1);
+            d = pair_den(pa, pc, pair_kind(pa, pc));
+        }
+        acc.canonical().store(prefix + ((u64)k * nthr + t) * 8);
+        acc = fmul(acc, d);
+    }
+    acc.canonical().store(tot + t * 8);
+}
+
+// Down pass: with inv_tot[t] the inverse of the thread's product, walk the slots backwards
+// (d^-1 = acc * prefix, then acc *= d), add the pairs, carry the singles, write list r + 1.
+template <bool CODES>
+__global__ void __launch_bounds__(256, 2) pair_down_kernel(const Batch b, const u32 *bkt, const u32 *pts,
+                                                          const u32 *starts, const u32 *starts_next, u64 nb,
+                                                          u64 nthr, const u32 *prefix, const u32 *inv_tot,
+                                                          u32 *out_bkt, u32 *out_pts) {
+    const u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nthr) return;
+    const u64 E = starts[nb];
+    Fq acc = Fq::load(inv_tot + t * 8);
+    for (u32 k = KA / 2; k-- > 0;) {
+        const u64 e0 = 2 * (t + (u64)k * nthr);
+        if (e0 >= E) continue;
+        const u32 b0 = bkt[e0];
+        const u32 b1 = e0 + 1 < E ? bkt[e0 + 1] : EMPTY;
+        u32 c0;
+        const u32 *a0 = list_addr<CODES>(b, pts, e0, b0, c0);
+        G1A r = signed_point(a0, c0);
+        if (b1 == b0) {
+            u32 c1;
+            const u32 *a1 = list_addr<CODES>(b, pts, e0 + 1, b0, c1);
+            const G1A c = signed_point(a1, c1);
+            const u32 kind = pair_kind(r, c);
+            const Fq d = pair_den(r, c, kind);
+            const Fq inv = fmul(acc, Fq::load(prefix + ((u64)k * nthr + t) * 8));
+            acc = fmul(acc, d);
+            r = pair_sum(r, c, kind, inv);
+        } else if (b1 != EMPTY) {
+            // the slot's second point starts the next bucket: carried on its own
+            u32 c1;
+            const u32 *a1 = list_addr<CODES>(b, pts, e0 + 1, b1, c1);
+            const u32 s1 = starts[b1];
+            const u64 q1 = starts_next[b1] + ((e0 + 1 - s1 + (s1 & 1u)) >> 1);
+            signed_point(a1, c1).store(out_pts + q1 * 16);
+            out_bkt[q1] = b1;
+        }
+        const u32 s0 = starts[b0];
+        const u64 q0 = starts_next[b0] + ((e0 - s0 + (s0 & 1u)) >> 1);
+        r.store(out_pts + q0 * 16);
+        out_bkt[q0] = b0;
+    }
+}
+
+// Montgomery's trick over a plain array of non-zero Fq values (the thread totals), in place.
+// A CTA takes TREE_SPAN values: thread j folds the values base + j + TREE_CTA k (k <
+// TREE_PER) into running prefixes and a product p_j; shared-memory scans give every thread the
+// products E_j of the threads before it and S_j of those after it, so p_j^-1 = P^-1 E_j S_j
+// with P the CTA's product.  tree_up_kernel hands P to the next level; tree_top_kernel (one
+// CTA, at most TREE_SPAN values) inverts its P once and resolves its members; tree_down_kernel
+// resolves a level's members from the inverses of its CTA products.
+
+// exclusive product scan over the CTA's threads, forward (reverse = false) or backward
+ZK_DI Fq cta_exclusive_product(const Fq &v, u32 *sm, bool reverse) {
+    const u32 j = reverse ? TREE_CTA - 1 - threadIdx.x : threadIdx.x;
+    Fq x = v;
+    for (u32 d = 1; d < TREE_CTA; d <<= 1) {
+        x.store(sm + j * 8);
+        __syncthreads();
+        const Fq y = j >= d ? Fq::load(sm + (j - d) * 8) : Fq::one();
+        __syncthreads();
+        x = fmul(x, y);
+    }
+    // x = inclusive product; shift by one
+    x.store(sm + j * 8);
+    __syncthreads();
+    const Fq r = j > 0 ? Fq::load(sm + (j - 1) * 8) : Fq::one();
+    __syncthreads();
+    return r;
+}
+
+// thread's member fold: pre[i] = product of its earlier members, returns the product
+ZK_DI Fq tree_fold(const u32 *vals, u64 n, u64 base, u32 *pre) {
+    Fq acc = Fq::one();
+    for (u32 k = 0; k < TREE_PER; k++) {
+        const u64 i = base + threadIdx.x + (u64)k * TREE_CTA;
+        if (i >= n) break;
+        acc.canonical().store(pre + i * 8);
+        acc = fmul(acc, Fq::load(vals + i * 8));
+    }
+    return acc;
+}
+
+// members from the inverse of the thread's product, walking backwards
+ZK_DI void tree_resolve(u32 *vals, u64 n, u64 base, const u32 *pre, Fq inv) {
+    for (u32 k = TREE_PER; k-- > 0;) {
+        const u64 i = base + threadIdx.x + (u64)k * TREE_CTA;
+        if (i >= n) continue;
+        const Fq v = Fq::load(vals + i * 8);
+        fmul(inv, Fq::load(pre + i * 8)).canonical().store(vals + i * 8);
+        inv = fmul(inv, v);
+    }
+}
+
+__global__ void __launch_bounds__(TREE_CTA) tree_up_kernel(const u32 *vals, u64 n, u32 *pre, u32 *ex, u32 *sx,
+                                                          u32 *tot) {
+    __shared__ __align__(16) u32 sm[TREE_CTA * 8];
+    const u64 base = (u64)blockIdx.x * TREE_SPAN;
+    const Fq p = tree_fold(vals, n, base, pre);
+    const Fq e = cta_exclusive_product(p, sm, false);
+    const Fq f = cta_exclusive_product(p, sm, true);
+    const u64 slot = (u64)blockIdx.x * TREE_CTA + threadIdx.x;
+    e.canonical().store(ex + slot * 8);
+    f.canonical().store(sx + slot * 8);
+    if (threadIdx.x == TREE_CTA - 1) fmul(e, p).canonical().store(tot + (u64)blockIdx.x * 8);
+}
+
+__global__ void __launch_bounds__(TREE_CTA) tree_top_kernel(u32 *vals, u64 n, u32 *pre) {
+    __shared__ __align__(16) u32 sm[TREE_CTA * 8];
+    const Fq p = tree_fold(vals, n, 0, pre);
+    const Fq e = cta_exclusive_product(p, sm, false);
+    const Fq f = cta_exclusive_product(p, sm, true);
+    if (threadIdx.x == TREE_CTA - 1) inv_binary<FqParams>(fmul(e, p)).store(sm);
+    __syncthreads();
+    const Fq inv_all = Fq::load(sm);
+    tree_resolve(vals, n, 0, pre, fmul(inv_all, fmul(e, f)));
+}
+
+__global__ void __launch_bounds__(TREE_CTA) tree_down_kernel(u32 *vals, u64 n, const u32 *pre, const u32 *ex,
+                                                            const u32 *sx, const u32 *inv_tot) {
+    const u64 base = (u64)blockIdx.x * TREE_SPAN;
+    const u64 slot = (u64)blockIdx.x * TREE_CTA + threadIdx.x;
+    const Fq inv = fmul(Fq::load(inv_tot + (u64)blockIdx.x * 8), fmul(Fq::load(ex + slot * 8), Fq::load(sx + slot * 8)));
+    tree_resolve(vals, n, base, pre, inv);
 }
 
 // ------------------------------------------------------------------ 5: bucket reduction
@@ -637,8 +973,9 @@ inline u32 grid_for(u64 items, u32 block, u32 per_sm = 8) {
 
 // Runs a batch of MSMs whose points / scalars are on the device; `ws` holds the layout
 // regions.  Launches only: no allocation, no host copy.
-// points_ready (optional): the accumulation waits for it, so a host-to-device copy of the
-// points can overlap the digit sort.  scalars_read (optional): recorded once the scalars have
+// points_ready (optional): the first kernel that reads the points (the first pairing round, or
+// the accumulation) waits for it, so a host-to-device copy of the points can overlap the
+// digit sort.  scalars_read (optional): recorded once the scalars have
 // been read (after the scatter), so the caller may overwrite them.
 cudaError_t run_batch(const Batch &b, const Layout &l, char *ws, cudaStream_t stream,
                       cudaEvent_t points_ready = nullptr, cudaEvent_t scalars_read = nullptr) {
@@ -656,6 +993,16 @@ cudaError_t run_batch(const Batch &b, const Layout &l, char *ws, cudaStream_t st
     u32 *cls = reinterpret_cast<u32 *>(ws + l.cls);
     u32 *win = reinterpret_cast<u32 *>(ws + l.win);
     const u64 nb = l.nb;
+    auto at = [&](size_t off) { return reinterpret_cast<u32 *>(ws + off); };
+    // exclusive scan of items counters in[] into out[] (and out2[])
+    auto scan = [&](const u32 *in, u64 items, u32 *out, u32 *out2) -> cudaError_t {
+        const u32 nblocks = (u32)((items + SCAN_BLOCK * SCAN_ITEMS - 1) / (SCAN_BLOCK * SCAN_ITEMS));
+        u32 *block_sums = at(l.scan_sums);
+        scan_reduce_kernel<<<nblocks, SCAN_BLOCK, 0, stream>>>(in, items, block_sums);
+        scan_blocks_kernel<<<1, SCAN_BLOCK, 0, stream>>>(block_sums, nblocks);
+        scan_apply_kernel<<<nblocks, SCAN_BLOCK, 0, stream>>>(in, items, block_sums, out, out2);
+        return cudaGetLastError();
+    };
 
     StageProfiler &prof = profiler();
     prof.begin(stream);
@@ -672,13 +1019,7 @@ cudaError_t run_batch(const Batch &b, const Layout &l, char *ws, cudaStream_t st
     prof.mark("count", stream);
     // exclusive scan of the nb + 1 counters: cursor[k] = first slot of bucket k, and
     // counts[nb] becomes the number of live (non-zero digit) entries
-    const u64 items = nb + 1;
-    const u32 nblocks = (u32)((items + SCAN_BLOCK * SCAN_ITEMS - 1) / (SCAN_BLOCK * SCAN_ITEMS));
-    u32 *block_sums = reinterpret_cast<u32 *>(ws + l.part_pts);  // free until accumulation
-    scan_reduce_kernel<<<nblocks, SCAN_BLOCK, 0, stream>>>(counts, items, block_sums);
-    scan_blocks_kernel<<<1, SCAN_BLOCK, 0, stream>>>(block_sums, nblocks);
-    scan_apply_kernel<<<nblocks, SCAN_BLOCK, 0, stream>>>(counts, items, block_sums, cursor, counts);
-    ZK_TRY(cudaGetLastError());
+    ZK_TRY(scan(counts, nb + 1, cursor, counts));
     prof.mark("scan", stream);
     if (scalars) {
         scatter_kernel<<<grid_for(scalars, 256), 256, 0, stream>>>(b, cursor, sb, sp);
@@ -688,8 +1029,75 @@ cudaError_t run_batch(const Batch &b, const Layout &l, char *ws, cudaStream_t st
     if (scalars_read) ZK_TRY(cudaEventRecord(scalars_read, stream));
     if (points_ready) ZK_TRY(cudaStreamWaitEvent(stream, points_ready, 0));
     const u32 *live = counts + nb;
+    const u32 *walk_bkt = sb, *walk_pts = sp;
+    static const char *const kUp[MAX_ROUNDS] = {"pair_up0", "pair_up1", "pair_up2", "pair_up3"};
+    static const char *const kTree[MAX_ROUNDS] = {"pair_tree0", "pair_tree1", "pair_tree2", "pair_tree3"};
+    static const char *const kDown[MAX_ROUNDS] = {"pair_down0", "pair_down1", "pair_down2", "pair_down3"};
+    for (u32 r = 0; r < l.rounds; r++) {
+        // list r + 1's bucket starts
+        const u32 *st = at(l.starts[r]);
+        u32 *st_next = at(l.starts[r + 1]);
+        halve_counts_kernel<<<(u32)((nb + 256) / 256), 256, 0, stream>>>(st, nb, cursor);
+        ZK_TRY(cudaGetLastError());
+        ZK_TRY(scan(cursor, nb + 1, st_next, st_next));
+        // Montgomery's trick over the round's pairs
+        const u64 T = l.thr[r];
+        const u32 grid = (u32)((T + 255) / 256);
+        u32 *prefix = at(l.prefix[r]), *tv = at(l.tvals);
+        u32 *out_bkt = at(l.lst_bkt[r % 2]), *out_pts = at(l.lst_pts[r % 2]);
+        if (r == 0)
+            pair_up_kernel<true><<<grid, 256, 0, stream>>>(b, walk_bkt, walk_pts, st, nb, T, prefix, tv);
+        else
+            pair_up_kernel<false><<<grid, 256, 0, stream>>>(b, walk_bkt, walk_pts, st, nb, T, prefix, tv);
+        ZK_TRY(cudaGetLastError());
+        prof.mark(kUp[r], stream);
+        // batched inverse of the T thread totals (levels as laid out for round 0's count)
+        {
+            u64 sizes[TREE_LEVELS + 1];
+            u32 *dat[TREE_LEVELS + 1];
+            u32 L = 0;
+            sizes[0] = T;
+            dat[0] = tv;
+            while (sizes[L] > TREE_SPAN) {
+                if (L == TREE_LEVELS) return cudaErrorInvalidValue;  // beyond the laid-out levels
+                const u64 ctas = (sizes[L] + TREE_SPAN - 1) / TREE_SPAN;
+                tree_up_kernel<<<(u32)ctas, TREE_CTA, 0, stream>>>(dat[L], sizes[L], at(l.tree_pre[L]),
+                                                                   at(l.tree_ex[L]), at(l.tree_sx[L]),
+                                                                   at(l.tree_dat[L + 1]));
+                ZK_TRY(cudaGetLastError());
+                dat[L + 1] = at(l.tree_dat[L + 1]);
+                sizes[L + 1] = ctas;
+                L++;
+            }
+            tree_top_kernel<<<1, TREE_CTA, 0, stream>>>(dat[L], sizes[L], at(l.tree_pre[L]));
+            ZK_TRY(cudaGetLastError());
+            for (u32 k = L; k-- > 0;) {
+                tree_down_kernel<<<(u32)sizes[k + 1], TREE_CTA, 0, stream>>>(dat[k], sizes[k], at(l.tree_pre[k]),
+                                                                             at(l.tree_ex[k]), at(l.tree_sx[k]),
+                                                                             dat[k + 1]);
+                ZK_TRY(cudaGetLastError());
+            }
+        }
+        prof.mark(kTree[r], stream);
+        if (r == 0)
+            pair_down_kernel<true><<<grid, 256, 0, stream>>>(b, walk_bkt, walk_pts, st, st_next, nb, T, prefix, tv,
+                                                             out_bkt, out_pts);
+        else
+            pair_down_kernel<false><<<grid, 256, 0, stream>>>(b, walk_bkt, walk_pts, st, st_next, nb, T, prefix,
+                                                              tv, out_bkt, out_pts);
+        ZK_TRY(cudaGetLastError());
+        prof.mark(kDown[r], stream);
+        walk_bkt = out_bkt;
+        walk_pts = out_pts;
+        live = st_next + nb;
+    }
     if (l.chunks) {
-        accumulate_kernel<<<(u32)((l.chunks + 255) / 256), 256, 0, stream>>>(b, sb, sp, live, bs, pp, pb, pf);
+        if (l.rounds)
+            accumulate_kernel<false><<<(u32)((l.chunks + 255) / 256), 256, 0, stream>>>(b, walk_bkt, walk_pts, live,
+                                                                                       bs, pp, pb, pf);
+        else
+            accumulate_kernel<true><<<(u32)((l.chunks + 255) / 256), 256, 0, stream>>>(b, sb, sp, live, bs, pp,
+                                                                                      pb, pf);
         ZK_TRY(cudaGetLastError());
     }
     prof.mark("accumulate", stream);
@@ -767,14 +1175,15 @@ inline void resolve(u64 n, u32 window, u32 n_tables_hint, u32 *c, u32 *n_tables)
     *n_tables = nt;
 }
 
-inline Batch single(const u32 *points, u32 n_tables, const u32 *scalars, u64 n, u32 c, u32 *result) {
+inline Batch single(const u32 *points, u32 n_tables, const u32 *scalars, u64 n, u32 c, u32 *result,
+                    int rounds = -1) {
     Batch b{};
     b.ntasks = 1;
     b.task[0] = make_task(n, c, n_tables);
     b.task[0].points = points;
     b.task[0].scalars = scalars;
     b.task[0].result = result;
-    finish_batch(b);
+    finish_batch(b, rounds);
     return b;
 }
 
@@ -843,6 +1252,22 @@ extern "C" cudaError_t zkp_mont_probe(unsigned int blocks, unsigned int iters, u
 }
 
 extern "C" unsigned int zkp_msm_default_window(unsigned long long n) { return msm::default_window(n); }
+
+// pairing rounds an MSM of n points with this window and table count runs under the current
+// setting
+extern "C" unsigned int zkp_msm_rounds_for(unsigned long long n, unsigned int window, unsigned int n_tables) {
+    u32 c, nt;
+    msm::resolve(n ? n : 1, window, n_tables, &c, &nt);
+    return msm::single(nullptr, nt, nullptr, n, c, nullptr).rounds;
+}
+
+// affine pairing rounds for MSMs planned after this call: -1 = by size (the default), else
+// 0..4.  Workspace sizes depend on it, so size queries and runs must see the same setting.
+extern "C" cudaError_t zkp_msm_set_affine_rounds(int rounds) {
+    ZK_CHECK_ARG(rounds >= -1 && rounds <= (int)msm::MAX_ROUNDS);
+    msm::affine_rounds_setting() = rounds;
+    return cudaSuccess;
+}
 
 extern "C" unsigned long long zkp_msm_workspace_size(unsigned long long n, unsigned int window, unsigned int n_tables) {
     u32 c, nt;
@@ -1127,7 +1552,8 @@ extern "C" cudaError_t zkp_msm_device_noalloc(const unsigned int *points_d, unsi
     msm::resolve(n, window, n_tables, &c, &nt);
     ZK_CHECK_ARG(c >= 2 && c <= 24 && nt >= 1);
     ZK_CHECK_ARG(n * nt < (1ull << 31));
-    const msm::Batch b = msm::single(points_d, nt, scalars_d, n, c, result_d);
+    // no pairing rounds: their lists would not fit the fixed scratch
+    const msm::Batch b = msm::single(points_d, nt, scalars_d, n, c, result_d, 0);
     const msm::Layout l = msm::make_layout(b);
     // larger problems do not fit the fixed scratch: refuse instead of overrunning it
     if (l.total > kNoAllocScratchBytes) return cudaErrorInvalidValue;

@@ -119,6 +119,17 @@ def default_window(n: int) -> int:
     return int(_lib().zkp_msm_default_window(n))
 
 
+def rounds_for(n: int, window: int = 0, n_tables: int = 1) -> int:
+    """Pairing rounds an MSM of n points runs under the current setting."""
+    return int(_lib().zkp_msm_rounds_for(n, window, n_tables))
+
+
+def set_affine_rounds(rounds: int = -1) -> None:
+    """Affine pairing rounds for MSMs planned from now on (-1 = chosen by size).  Workspace
+    sizes depend on it: size and run under the same setting."""
+    check(_lib().zkp_msm_set_affine_rounds(int(rounds)), "zkp_msm_set_affine_rounds")
+
+
 class ResidentBases:
     """Bases kept in HBM (optionally with precomputed tables) for repeated MSMs: the
     device-pointer form the served path uses."""

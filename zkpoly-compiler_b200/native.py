@@ -56,6 +56,8 @@ SIGNATURES = {
         "msm_precompute": (cudaError_t, [ctypes.c_ulonglong, ctypes.POINTER(c_void_p), ctypes.c_uint]),
         "zkp_msm_workspace_size": (ctypes.c_ulonglong, [ctypes.c_ulonglong, ctypes.c_uint, ctypes.c_uint]),
         "zkp_msm_default_window": (ctypes.c_uint, [ctypes.c_ulonglong]),
+        "zkp_msm_set_affine_rounds": (cudaError_t, [ctypes.c_int]),
+        "zkp_msm_rounds_for": (ctypes.c_uint, [ctypes.c_ulonglong, ctypes.c_uint, ctypes.c_uint]),
         "zkp_msm_device": (cudaError_t, [c_void_p, ctypes.c_ulonglong, c_void_p, ctypes.c_uint, c_void_p,
                                          ctypes.c_ulonglong, ctypes.c_uint, c_void_p, c_void_p]),
         "zkp_msm_precompute_device": (cudaError_t, [c_void_p, ctypes.c_ulonglong, ctypes.c_uint, ctypes.c_uint,
