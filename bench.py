@@ -199,6 +199,8 @@ def run_gpu(args):
             win, nt = zk.tuner.msm_resident_config(n_msm)
             if args.tables:
                 nt = args.tables
+        if args.msm_rounds >= 0:
+            zk.msm.set_affine_rounds(args.msm_rounds)
         bases = zk.msm.ResidentBases(points, window=win, n_tables=nt)
         ws = bases.workspace()
         res = torch.zeros(16, dtype=torch.int32, device=dev)
@@ -629,6 +631,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--window", type=int, default=0)
     ap.add_argument("--tables", type=int, default=0, help="precomputed point tables (0 = tuned / full)")
+    ap.add_argument("--msm-rounds", type=int, default=-1,
+                    help="affine pairing rounds of the MSM (-1 = the library's choice by size)")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-fused", action="store_true")
     ap.add_argument("--no-served", action="store_true")

@@ -292,3 +292,81 @@ def test_reference_poly_library_matches(zk, log_n):
             ms_ref, ms = _event_ms(run_ref), _event_ms(run)
             print(json.dumps({"compare": name, "log_n": log_n, "reference_ms": ms_ref, "this_ms": ms,
                               "speedup": ms_ref / ms}))
+
+
+def test_reference_batched_workload_per_call(zk):
+    """Config 4's workload (seed 3: 64 NTTs 2^10..2^20 of mixed kinds, 16 MSMs 2^12..2^22)
+    through the reference's own kernels one call at a time - ssip_ntt, with distribute_powers
+    for the inverse's n^-1 and the coset's g^i (the compiler's composition), and the
+    reference-ABI msm with host arrays from libref_msm_17_8 (its cost model's 2^22
+    configuration, two tables built by msm_precompute per size) - must give this repository's
+    batched results; with ZKP_REF_TIMING=1 both sides are timed."""
+    ref_ntt = _ref_ntt(zk)
+    ref_ntt.distribute_powers.restype = ctypes.c_int
+    ref_ntt.distribute_powers.argtypes = [zk.native.PolyPtr, ctypes.c_void_p, ctypes.c_ulonglong, ctypes.c_void_p]
+    ref_msm = _ref_msm("libref_msm_17_8.so")
+    w = zk.batched.MixedWorkload(seed=3)
+    w.build_batched()
+    w.reset_inputs()
+    w.run_batched()
+    torch.cuda.synchronize()
+    ntt_ours, msm_ours = w.snapshot()
+    st = torch.cuda.current_stream().cuda_stream
+    # reference-side set-up (untimed): twiddles, inverse scales, coset powers, point tables
+    tw = {(L, inv): zk.ntt.twiddle_table(L, inv) for L in set(w.ntt_logs) for inv in (False, True)}
+    ninv = {L: zk.ntt.n_inv(L) for L in set(w.ntt_logs)}
+    coset = {}
+    for L, kind in zip(w.ntt_logs, w.ntt_kinds):
+        if kind == "coset" and L not in coset:
+            p = zk.ntt.scalar_const(7).repeat(1 << L, 1)
+            p[0] = zk.ntt.scalar_const(1)[0]
+            pa = zk.ScalarArray(p)
+            zk.poly.scan_mul(pa)  # g^i
+            coset[L] = pa
+    tables = {}
+    for L in set(w.msm_logs):
+        n = 1 << L
+        t = [_pinned_u32(w.bases[:n]), np.zeros((n, 16), dtype=np.uint32)]
+        h_tab = (ctypes.c_void_p * 2)(*[a.ctypes.data for a in t])
+        assert ref_msm.msm_precompute(n, h_tab, 1) == 0
+        tables[L] = t
+    h_scal = [_pinned_u32(s) for s in w.scalars]
+    bufs = [zk.ScalarArray(t.clone()) for t in w.ntt_init]
+    torch.cuda.synchronize()
+
+    def run_reference():
+        for x, t0, L, kind in zip(bufs, w.ntt_init, w.ntt_logs, w.ntt_kinds):
+            x.values.copy_(t0)
+            if kind == "coset":
+                assert ref_ntt.distribute_powers(x.poly_ptr(), coset[L].values.data_ptr(), 1 << L, st) == 0
+            assert ref_ntt.ssip_ntt(x.poly_ptr(), tw[(L, kind == "intt")].values.data_ptr(), L, st, 8, 8) == 0
+            if kind == "intt":
+                assert ref_ntt.distribute_powers(x.poly_ptr(), ninv[L].data_ptr(), 1, st) == 0
+        out = []
+        for hs, L in zip(h_scal, w.msm_logs):
+            n = 1 << L
+            parts = 16 if n >= (1 << 16) else 1
+            res, _ = _call_msm(ref_msm, n, tables[L], [hs], parts=parts, stages=2 if parts > 1 else 1)
+            out.append(res[0])
+        torch.cuda.synchronize()
+        return out
+
+    msm_ref = run_reference()
+    for a, b in zip(bufs, ntt_ours):
+        assert torch.equal(a.values, b)
+    for a, b in zip(msm_ref, msm_ours):
+        assert np.array_equal(a, b.cpu().numpy().view(np.uint32))
+    if TIMING:
+        t0 = time.perf_counter()
+        run_reference()
+        ref_ms = (time.perf_counter() - t0) * 1e3
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(3):
+            w.run_batched()
+        e1.record()
+        torch.cuda.synchronize()
+        batched_ms = e0.elapsed_time(e1) / 3
+        print(json.dumps({"compare": "config-4 workload", "reference_per_call_ms": ref_ms,
+                          "this_batched_ms": batched_ms, "speedup": ref_ms / batched_ms}))
