@@ -705,7 +705,7 @@ __global__ void __launch_bounds__(256) pair_up_kernel(const Batch b, const u32 *
 // Down pass: with inv_tot[t] the inverse of the thread's product, walk the slots backwards
 // (d^-1 = acc * prefix, then acc *= d), add the pairs, carry the singles, write list r + 1.
 template <bool CODES>
-__global__ void __launch_bounds__(256, 2) pair_down_kernel(const Batch b, const u32 *bkt, const u32 *pts,
+__global__ void __launch_bounds__(256, 3) pair_down_kernel(const Batch b, const u32 *bkt, const u32 *pts,
                                                           const u32 *starts, const u32 *starts_next, u64 nb,
                                                           u64 nthr, const u32 *prefix, const u32 *inv_tot,
                                                           u32 *out_bkt, u32 *out_pts) {
