@@ -125,7 +125,9 @@ inline int &affine_rounds_setting() {
     static int r = -1;
     return r;
 }
-inline u32 auto_rounds(u64 entries) { return entries >= (1ull << 24) ? 3u : 0u; }
+inline u32 auto_rounds(u64 entries) {
+    return entries >= (1ull << 26) ? 4u : (entries >= (1ull << 24) ? 3u : 0u);
+}
 
 // upper bounds of the list lengths: E_0 = live digits, E_{r+1} <= sum_b (m_b / 2 + 1) =
 // E_r / 2 + nb (a bucket's run leaves at most one unpaired point at each end)
