@@ -213,8 +213,9 @@ inline Layout make_layout(const Batch &b) {
     l.counts = take((l.nb + 1) * 4);
     l.cursor = take((l.nb + 1) * 4);
     l.scan_sums = take(((l.nb + 1) / 4096 + 2) * 4);
-    l.sorted_bucket = take(l.entries * 4);
-    l.sorted_point = take(l.entries * 4);
+    // list 0: one 8-byte record per digit (bucket id, point code), written by one store
+    l.sorted_bucket = take(l.entries * 8);
+    l.sorted_point = l.sorted_bucket + 4;
     if (l.rounds) {
         l.starts[0] = l.counts;
         for (u32 r = 1; r <= l.rounds; r++) l.starts[r] = take((l.nb + 1) * 4);
@@ -229,7 +230,7 @@ inline Layout make_layout(const Batch &b) {
         l.prefix[0] = (l.rounds >= 2 && pre0 <= l.emax[2] * 64) ? l.lst_pts[1] : take(pre0);
         if (l.rounds >= 2) {
             const u64 pre1 = l.thr[1] * (KA / 2) * 32;  // thr[r] <= thr[1] for r >= 1
-            const size_t sorted_bytes = l.sorted_point + l.entries * 4 - l.sorted_bucket;
+            const size_t sorted_bytes = l.entries * 8;
             const size_t at1 = pre1 <= sorted_bytes ? l.sorted_bucket : take(pre1);
             for (u32 r = 1; r < l.rounds; r++) l.prefix[r] = at1;
         }
@@ -326,8 +327,7 @@ __global__ void __launch_bounds__(256) count_kernel(const Batch b, u32 *counts) 
     }
 }
 
-__global__ void __launch_bounds__(256) scatter_kernel(const Batch b, u32 *cursor, u32 *sorted_bucket,
-                                                     u32 *sorted_point) {
+__global__ void __launch_bounds__(256) scatter_kernel(const Batch b, u32 *cursor, uint2 *records) {
     const u64 total = b.sc_first[b.ntasks];
     const u64 stride = (u64)gridDim.x * blockDim.x;
     for (u64 g = (u64)blockIdx.x * blockDim.x + threadIdx.x; g < total; g += stride) {
@@ -339,8 +339,7 @@ __global__ void __launch_bounds__(256) scatter_kernel(const Batch b, u32 *cursor
         load_digits(d, k.scalars + i * 8, k.c);
         for_each_digit(d, k, [&](u32 table, u32 key, bool neg) {
             const u32 pos = atomicAdd(cursor + kb + key, 1u);
-            sorted_bucket[pos] = kb + key;
-            sorted_point[pos] = (u32)(table * k.stride + i) | (neg ? 0x80000000u : 0u);
+            records[pos] = make_uint2(kb + key, (u32)(table * k.stride + i) | (neg ? 0x80000000u : 0u));
         });
     }
 }
@@ -438,23 +437,25 @@ ZK_DI G1A fetch_point(const u32 *points, u32 code) {
 #ifndef ZK_ACC_MIN_BLOCKS
 #define ZK_ACC_MIN_BLOCKS 2  // resident CTAs of 256 threads per SM the register budget targets
 #endif
-// CODES: the walk reads list 0 (point codes into the task tables); otherwise the explicit
-// points of the last pairing round's list, at their list positions.
+// CODES: the walk reads list 0 (8-byte records: bucket id, point code into the task tables;
+// sorted_point = sorted_bucket + 1, stride 2 words); otherwise the last pairing round's list
+// (bucket ids, and explicit points at their list positions).
 template <bool CODES>
 __global__ void __launch_bounds__(256, ZK_ACC_MIN_BLOCKS) accumulate_kernel(const Batch b, const u32 *sorted_bucket,
                                                            const u32 *sorted_point, const u32 *live,
                                                            u32 *bucket_sums, u32 *part_pts, u32 *part_bucket,
                                                            u32 *part_flag) {
+    constexpr u32 S = CODES ? 2 : 1;  // words between consecutive bucket ids
     const u64 entries = *live;
     const u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x;
     const u64 start = t * b.K;
     if (start >= entries) return;
     const u64 end = start + b.K < entries ? start + b.K : entries;
-    const bool from_prev = start > 0 && sorted_bucket[start - 1] == sorted_bucket[start];
+    const bool from_prev = start > 0 && sorted_bucket[S * (start - 1)] == sorted_bucket[S * start];
     u64 run_start = start;
-    u32 cur = sorted_bucket[start];
+    u32 cur = sorted_bucket[S * start];
     const u32 *pts = CODES ? b.task[find_task(b.key_first, b.ntasks, (u64)cur)].points : sorted_point;
-    G1X acc = G1X::from_affine(CODES ? fetch_point(pts, sorted_point[start])
+    G1X acc = G1X::from_affine(CODES ? fetch_point(pts, sorted_point[S * start])
                                      : G1A::load_nc(sorted_point + start * 16));
     // The next record's bucket, code and point address are read one iteration ahead; its point
     // is loaded when it is used.  (Keeping the point load itself one iteration ahead helped
@@ -464,9 +465,9 @@ __global__ void __launch_bounds__(256, ZK_ACC_MIN_BLOCKS) accumulate_kernel(cons
     const u32 *npts = pts;
     const u32 *naddr = pts;
     if (start + 1 < end) {
-        nbk = sorted_bucket[start + 1];
+        nbk = sorted_bucket[S * (start + 1)];
         if (CODES) {
-            ncode = sorted_point[start + 1];
+            ncode = sorted_point[S * (start + 1)];
             if (nbk != cur) npts = b.task[find_task(b.key_first, b.ntasks, (u64)nbk)].points;
             naddr = npts + (u64)(ncode & 0x7fffffffu) * 16;
         } else {
@@ -479,9 +480,9 @@ __global__ void __launch_bounds__(256, ZK_ACC_MIN_BLOCKS) accumulate_kernel(cons
         G1A pt;
         if (p < end) pt = G1A::load_nc(naddr);
         if (p + 1 < end) {
-            nbk = sorted_bucket[p + 1];
+            nbk = sorted_bucket[S * (p + 1)];
             if (CODES) {
-                ncode = sorted_point[p + 1];
+                ncode = sorted_point[S * (p + 1)];
                 if (nbk != bk) npts = b.task[find_task(b.key_first, b.ntasks, (u64)nbk)].points;
                 naddr = npts + (u64)(ncode & 0x7fffffffu) * 16;
             } else {
@@ -496,7 +497,7 @@ __global__ void __launch_bounds__(256, ZK_ACC_MIN_BLOCKS) accumulate_kernel(cons
             continue;
         }
         const bool head = run_start == start && from_prev;
-        const bool to_next = p == end && end < entries && sorted_bucket[end] == cur;
+        const bool to_next = p == end && end < entries && sorted_bucket[S * end] == cur;
         if (!head && !to_next) {
             acc.store(bucket_sums + (u64)cur * 32);
         } else {
@@ -615,12 +616,12 @@ __global__ void halve_counts_kernel(const u32 *starts, u64 nb, u32 *cnt) {
 
 
 // Address of the point at list position e, and its sign code.  CODES: list 0, whose entries
-// are point codes into the bucket's task tables (index | sign << 31); otherwise explicit
-// 64-byte canonical affine points.
+// are 8-byte records (bucket id, point code into the bucket's task tables: index | sign << 31;
+// pts = the record array + 1 word); otherwise explicit 64-byte canonical affine points.
 template <bool CODES>
 ZK_DI const u32 *list_addr(const Batch &b, const u32 *pts, u64 e, u32 bucket, u32 &code) {
     if (CODES) {
-        code = pts[e];
+        code = pts[2 * e];
         const u32 *tbl = b.task[find_task(b.key_first, b.ntasks, (u64)bucket)].points;
         return tbl + (u64)(code & 0x7fffffffu) * 16;
     }
@@ -678,6 +679,7 @@ ZK_DI G1A pair_sum(const G1A &a, const G1A &c, u32 kind, const Fq &inv) {
 template <bool CODES>
 __global__ void __launch_bounds__(256) pair_up_kernel(const Batch b, const u32 *bkt, const u32 *pts,
                                                      const u32 *starts, u64 nb, u64 nthr, u32 *prefix, u32 *tot) {
+    constexpr u32 S = CODES ? 2 : 1;  // words between consecutive bucket ids
     const u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nthr) return;
     const u64 E = starts[nb];
@@ -685,8 +687,8 @@ __global__ void __launch_bounds__(256) pair_up_kernel(const Batch b, const u32 *
     for (u32 k = 0; k < KA / 2; k++) {
         const u64 e0 = 2 * (t + (u64)k * nthr);
         if (e0 + 1 >= E) break;
-        const u32 b0 = bkt[e0];
-        if (bkt[e0 + 1] != b0) continue;
+        const u32 b0 = bkt[S * e0];
+        if (bkt[S * (e0 + 1)] != b0) continue;
         u32 c0, c1;
         const u32 *a0 = list_addr<CODES>(b, pts, e0, b0, c0);
         const u32 *a1 = list_addr<CODES>(b, pts, e0 + 1, b0, c1);
@@ -711,6 +713,7 @@ __global__ void __launch_bounds__(256, 3) pair_down_kernel(const Batch b, const 
                                                           const u32 *starts, const u32 *starts_next, u64 nb,
                                                           u64 nthr, const u32 *prefix, const u32 *inv_tot,
                                                           u32 *out_bkt, u32 *out_pts) {
+    constexpr u32 S = CODES ? 2 : 1;  // words between consecutive bucket ids
     const u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nthr) return;
     const u64 E = starts[nb];
@@ -718,8 +721,8 @@ __global__ void __launch_bounds__(256, 3) pair_down_kernel(const Batch b, const 
     for (u32 k = KA / 2; k-- > 0;) {
         const u64 e0 = 2 * (t + (u64)k * nthr);
         if (e0 >= E) continue;
-        const u32 b0 = bkt[e0];
-        const u32 b1 = e0 + 1 < E ? bkt[e0 + 1] : EMPTY;
+        const u32 b0 = bkt[S * e0];
+        const u32 b1 = e0 + 1 < E ? bkt[S * (e0 + 1)] : EMPTY;
         u32 c0;
         const u32 *a0 = list_addr<CODES>(b, pts, e0, b0, c0);
         G1A r = signed_point(a0, c0);
@@ -1024,7 +1027,7 @@ cudaError_t run_batch(const Batch &b, const Layout &l, char *ws, cudaStream_t st
     ZK_TRY(scan(counts, nb + 1, cursor, counts));
     prof.mark("scan", stream);
     if (scalars) {
-        scatter_kernel<<<grid_for(scalars, 256), 256, 0, stream>>>(b, cursor, sb, sp);
+        scatter_kernel<<<grid_for(scalars, 256), 256, 0, stream>>>(b, cursor, reinterpret_cast<uint2 *>(sb));
         ZK_TRY(cudaGetLastError());
     }
     prof.mark("scatter", stream);
