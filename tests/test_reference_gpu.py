@@ -357,9 +357,11 @@ def test_reference_batched_workload_per_call(zk):
     for a, b in zip(msm_ref, msm_ours):
         assert np.array_equal(a, b.cpu().numpy().view(np.uint32))
     if TIMING:
-        t0 = time.perf_counter()
-        run_reference()
-        ref_ms = (time.perf_counter() - t0) * 1e3
+        ref_ms = float("inf")
+        for _ in range(3):  # best of three: the reference's msm allocates and frees per call
+            t0 = time.perf_counter()
+            run_reference()
+            ref_ms = min(ref_ms, (time.perf_counter() - t0) * 1e3)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
