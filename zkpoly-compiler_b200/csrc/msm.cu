@@ -175,6 +175,7 @@ constexpr u32 TREE_LEVELS = 3;
 
 struct Layout {
     size_t counts, cursor, sorted_bucket, sorted_point, bucket_sums, part_pts, part_bucket, part_flag, long_list,
+        chain_list,
         seg, cls, win, scan_sums, total;
     u64 nb, entries, chunks, segs, wins;
     // affine pairing rounds: list r + 1 (r < rounds) lives in buffer r % 2; starts[r] are the
@@ -251,7 +252,8 @@ inline Layout make_layout(const Batch &b) {
     l.part_pts = take(l.chunks * 2 * 128);
     l.part_bucket = take(l.chunks * 2 * 4);
     l.part_flag = take(l.chunks * 2 * 4);
-    l.long_list = take((l.chunks + 1) * 4 + 4);  // chain starts + a counter at the end
+    l.long_list = take((l.chunks + 1) * 4 + 4);  // long chain starts + a counter at the end
+    l.chain_list = take((l.chunks + 1) * 4);     // chain starts + a counter at the end
     l.seg = take(2 * l.segs * 128);  // U_g then T_g
     l.cls = take(l.wins * b.ncls * b.nparts * 128);
     l.win = take(l.wins * 128);
@@ -444,7 +446,7 @@ template <bool CODES>
 __global__ void __launch_bounds__(256, ZK_ACC_MIN_BLOCKS) accumulate_kernel(const Batch b, const u32 *sorted_bucket,
                                                            const u32 *sorted_point, const u32 *live,
                                                            u32 *bucket_sums, u32 *part_pts, u32 *part_bucket,
-                                                           u32 *part_flag) {
+                                                           u32 *part_flag, u32 *chain_list, u32 *chain_count) {
     constexpr u32 S = CODES ? 2 : 1;  // words between consecutive bucket ids
     const u64 entries = *live;
     const u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x;
@@ -464,6 +466,7 @@ __global__ void __launch_bounds__(256, ZK_ACC_MIN_BLOCKS) accumulate_kernel(cons
     u32 nbk = EMPTY, ncode = 0;
     const u32 *npts = pts;
     const u32 *naddr = pts;
+    bool chain_start = false;  // a tail partial was written: a chain for the fix-up starts here
     if (start + 1 < end) {
         nbk = sorted_bucket[S * (start + 1)];
         if (CODES) {
@@ -505,6 +508,7 @@ __global__ void __launch_bounds__(256, ZK_ACC_MIN_BLOCKS) accumulate_kernel(cons
             acc.store(part_pts + slot * 32);
             part_bucket[slot] = cur;
             part_flag[slot] = head ? (to_next ? 2u : 1u) : 3u;
+            chain_start = chain_start || !head;
         }
         if (p < end) {
             cur = bk;
@@ -512,6 +516,17 @@ __global__ void __launch_bounds__(256, ZK_ACC_MIN_BLOCKS) accumulate_kernel(cons
             pts = bpts;
             acc = G1X::from_affine(pt);
         }
+    }
+    // append this chunk to the fix-up's list of chain starts (one atomic per group of lanes
+    // that arrive together), so that the fix-up runs dense threads
+    const unsigned act = __activemask();
+    const unsigned want = __ballot_sync(act, chain_start);
+    if (want) {
+        const u32 lane = threadIdx.x & 31, leader = __ffs(want) - 1;
+        u32 base = 0;
+        if (lane == leader) base = atomicAdd(chain_count, (u32)__popc(want));
+        base = __shfl_sync(act, base, leader);
+        if (chain_start) chain_list[base + __popc(want & ((1u << lane) - 1u))] = (u32)t;
     }
 }
 
@@ -527,12 +542,15 @@ ZK_DI bool chain_member(const u32 *part_bucket, const u32 *part_flag, u64 u, u32
     return (f == 1u || f == 2u) && part_bucket[2 * u] == bucket;
 }
 
+// One thread per chain start recorded by the walk (chain_list, chain_count entries).
 __global__ void __launch_bounds__(256) fixup_kernel(const u32 *live, u32 K, u32 *bucket_sums, const u32 *part_pts,
-                                                   const u32 *part_bucket, const u32 *part_flag, u32 *long_list,
+                                                   const u32 *part_bucket, const u32 *part_flag,
+                                                   const u32 *chain_list, const u32 *chain_count, u32 *long_list,
                                                    u32 *long_count) {
     const u64 chunks = ((u64)*live + K - 1) / K;
-    const u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= chunks || part_flag[2 * t + 1] != 3u) return;
+    const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= *chain_count) return;
+    const u64 t = chain_list[i];
     const u64 slot = 2 * t + 1;
     const u32 bucket = part_bucket[slot];
     // a chain longer than SHORT_CHAIN goes to the CTA-wide pass
@@ -994,6 +1012,8 @@ cudaError_t run_batch(const Batch &b, const Layout &l, char *ws, cudaStream_t st
     u32 *pf = reinterpret_cast<u32 *>(ws + l.part_flag);
     u32 *longs = reinterpret_cast<u32 *>(ws + l.long_list);
     u32 *nlong = longs + l.chunks + 1;
+    u32 *chains = reinterpret_cast<u32 *>(ws + l.chain_list);
+    u32 *nchain = chains + l.chunks;
     u32 *seg = reinterpret_cast<u32 *>(ws + l.seg);
     u32 *cls = reinterpret_cast<u32 *>(ws + l.cls);
     u32 *win = reinterpret_cast<u32 *>(ws + l.win);
@@ -1015,6 +1035,7 @@ cudaError_t run_batch(const Batch &b, const Layout &l, char *ws, cudaStream_t st
     ZK_TRY(cudaMemsetAsync(bs, 0, nb * 128, stream));
     ZK_TRY(cudaMemsetAsync(pf, 0, l.chunks * 2 * 4, stream));
     ZK_TRY(cudaMemsetAsync(nlong, 0, 4, stream));
+    ZK_TRY(cudaMemsetAsync(nchain, 0, 4, stream));
     prof.mark("memset", stream);
     const u64 scalars = b.sc_first[b.ntasks];
     if (scalars) {
@@ -1099,15 +1120,17 @@ cudaError_t run_batch(const Batch &b, const Layout &l, char *ws, cudaStream_t st
     if (l.chunks) {
         if (l.rounds)
             accumulate_kernel<false><<<(u32)((l.chunks + 255) / 256), 256, 0, stream>>>(b, walk_bkt, walk_pts, live,
-                                                                                       bs, pp, pb, pf);
+                                                                                       bs, pp, pb, pf, chains,
+                                                                                       nchain);
         else
             accumulate_kernel<true><<<(u32)((l.chunks + 255) / 256), 256, 0, stream>>>(b, sb, sp, live, bs, pp,
-                                                                                      pb, pf);
+                                                                                      pb, pf, chains, nchain);
         ZK_TRY(cudaGetLastError());
     }
     prof.mark("accumulate", stream);
     if (l.chunks) {
-        fixup_kernel<<<(u32)((l.chunks + 255) / 256), 256, 0, stream>>>(live, b.K, bs, pp, pb, pf, longs, nlong);
+        fixup_kernel<<<(u32)((l.chunks + 255) / 256), 256, 0, stream>>>(live, b.K, bs, pp, pb, pf, chains, nchain,
+                                                                        longs, nlong);
         ZK_TRY(cudaGetLastError());
         long_chain_kernel<<<num_sms() * 2, 128, 0, stream>>>(live, b.K, bs, pp, pb, pf, longs, nlong);
         ZK_TRY(cudaGetLastError());
