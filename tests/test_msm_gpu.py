@@ -214,3 +214,17 @@ def test_msm_batch_affine_rounds(zk, orc):
             assert np.array_equal(t["result"].cpu().numpy().view(np.uint64), e)
     finally:
         zk.msm.set_affine_rounds(-1)
+
+
+@pytest.mark.parametrize("rounds", [0, 3])
+def test_msm_one_bucket_long_chains(zk, orc, rounds):
+    """2^16 equal scalars over full tables: every window's digits land in one bucket, whose run
+    spans many walk chunks (the fix-up's long-chain path), with and without pairing rounds."""
+    n = 1 << 16
+    s = np.repeat(orc.gen_fr(530, 1), n, axis=0)
+    p = orc.gen_points(531, n)
+    zk.msm.set_affine_rounds(rounds)
+    try:
+        assert np.array_equal(_device_msm(zk, s, p, 13, 20), orc.best_multiexp(s, p))
+    finally:
+        zk.msm.set_affine_rounds(-1)

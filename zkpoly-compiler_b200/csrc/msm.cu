@@ -85,6 +85,10 @@ ZK_DI u32 find_task(const T *first, u32 ntasks, T x) {
     return lo;
 }
 
+// CTAs per bit class in the bucket reduction (a power of two); the window kernel folds up to
+// 32 classes x 32 parts
+constexpr u32 MAX_PARTS = 32;
+
 inline Task make_task(u64 n, u32 c, u32 n_tables) {
     Task t{};
     t.n = n;
@@ -94,11 +98,14 @@ inline Task make_task(u64 n, u32 c, u32 n_tables) {
     t.n_tables = n_tables;
     t.Wp = (t.W + n_tables - 1) / n_tables;
     t.B = 1u << (c - 1);
-    t.L = t.B >= 8 ? 4 : t.B / 2;  // at least two segments per window
+    // buckets per reduction segment: 4, or more for large windows so that the bit classes stay
+    // small (8 at 2^19 buckets, 16 from 2^20); at least two segments per window
+    t.L = t.B >= 8 ? 4 : t.B / 2;
+    if (t.B >= (1u << 19)) t.L = t.B >= (1u << 20) ? 16 : 8;
     const u32 G = t.B / t.L;
     t.gbits = 31 - __builtin_clz(G);
     const u32 half = G / 2, per_cta = 256 * 8;  // about 8 additions per thread
-    t.parts = half / per_cta < 1 ? 1 : (half / per_cta > 8 ? 8 : half / per_cta);
+    t.parts = half / per_cta < 1 ? 1 : (half / per_cta > MAX_PARTS ? MAX_PARTS : half / per_cta);
     return t;
 }
 
@@ -927,12 +934,17 @@ __global__ void __launch_bounds__(256) window_kernel(const Batch b, const u32 *c
     const u32 t = find_task(b.win_first, b.ntasks, wg);
     const Task &k = b.task[t];
     const u32 ncls = k.gbits + 2, P = k.parts, tid = threadIdx.x;
+    // thread (class tid / 8, lane tid % 8) first sums the parts p = lane, lane + 8, ...; then a
+    // tree over the 8 lanes of each class
+    const u32 cl = tid >> 3, sub = tid & 7;
     G1X v = G1X::identity();
-    if (tid < ncls * P) v = G1X::load(cls_out + (((u64)wg * b.ncls + tid / P) * b.nparts + tid % P) * 32);
+    if (cl < ncls)
+        for (u32 p = sub; p < P; p += 8)
+            v = g1_add(v, G1X::load(cls_out + (((u64)wg * b.ncls + cl) * b.nparts + p) * 32));
     v.store(sm + tid * 32);
     __syncthreads();
-    for (u32 st = P / 2; st > 0; st >>= 1) {  // the parts of each class, P a power of two
-        if (tid < ncls * P && (tid % P) < st) {
+    for (u32 st = 4; st > 0; st >>= 1) {
+        if (cl < ncls && sub < st) {
             G1X x = G1X::load(sm + tid * 32);
             G1X y = G1X::load(sm + (tid + st) * 32);
             g1_add(x, y).store(sm + tid * 32);
@@ -941,7 +953,7 @@ __global__ void __launch_bounds__(256) window_kernel(const Batch b, const u32 *c
     }
     G1X x = G1X::identity();
     if (tid < ncls) {
-        x = G1X::load(sm + tid * P * 32);
+        x = G1X::load(sm + tid * 8 * 32);
         if (tid < k.gbits) {
             const u32 dbls = tid + (31 - __clz(k.L));  // 2^tid * L
             for (u32 i = 0; i < dbls; i++) x = g1_dbl(x);
