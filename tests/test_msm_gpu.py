@@ -228,3 +228,18 @@ def test_msm_one_bucket_long_chains(zk, orc, rounds):
         assert np.array_equal(_device_msm(zk, s, p, 13, 20), orc.best_multiexp(s, p))
     finally:
         zk.msm.set_affine_rounds(-1)
+
+
+def test_msm_affine_rounds_empty_lists(zk, orc):
+    """Pairing rounds over empty and near-empty digit lists: all-zero scalars (no live entries)
+    and a single non-zero scalar."""
+    n = 4096
+    p = orc.gen_points(540, n)
+    s = np.zeros((n, 4), dtype=np.uint64)
+    zk.msm.set_affine_rounds(3)
+    try:
+        assert np.array_equal(_device_msm(zk, s, p, 9), np.zeros(8, dtype=np.uint64))
+        s[1234] = orc.gen_fr(541, 1)[0]
+        assert np.array_equal(_device_msm(zk, s, p, 9), orc.best_multiexp(s, p))
+    finally:
+        zk.msm.set_affine_rounds(-1)
