@@ -109,9 +109,12 @@ inline Task make_task(u64 n, u32 c, u32 n_tables) {
     return t;
 }
 
-// default window width for n points (a cost model in the spirit of
-// core/src/msm/tuning/cost_model.py: n*W mixed adds vs 2*W*2^(c-1) bucket adds)
+// default window width for n points with one point table (a cost model in the spirit of
+// core/src/msm/tuning/cost_model.py: n*W mixed adds vs 2*W*2^(c-1) bucket adds).  From 2^18 to
+// 2^23 points the model is replaced by the width measured fastest on B200 with the pairing
+// rounds (one table: 15 at 2^18, 2^20 and 2^22, 3-4 % ahead of the model's 16 and 17).
 inline u32 default_window(u64 n) {
+    if (n >= (1ull << 18) && n <= (1ull << 23)) return 15;
     u32 best = 8;
     double best_cost = 1e300;
     for (u32 c = 8; c <= 20; c++) {
@@ -339,10 +342,13 @@ __global__ void __launch_bounds__(256) count_kernel(const Batch b, u32 *counts) 
     }
 }
 
-__global__ void __launch_bounds__(256) scatter_kernel(const Batch b, u32 *cursor, uint2 *records) {
-    const u64 total = b.sc_first[b.ntasks];
+// Scalars [first, last) of the batch's concatenation (one launch per task, so that the
+// records being written at any time fall into one task's buckets: with a whole batch at once the
+// open write positions of millions of buckets overflow L2).
+__global__ void __launch_bounds__(256) scatter_kernel(const Batch b, u32 *cursor, uint2 *records, u64 first,
+                                                     u64 last) {
     const u64 stride = (u64)gridDim.x * blockDim.x;
-    for (u64 g = (u64)blockIdx.x * blockDim.x + threadIdx.x; g < total; g += stride) {
+    for (u64 g = first + (u64)blockIdx.x * blockDim.x + threadIdx.x; g < last; g += stride) {
         const u32 t = find_task(b.sc_first, b.ntasks, g);
         const Task &k = b.task[t];
         const u64 i = g - b.sc_first[t];
@@ -1062,8 +1068,11 @@ cudaError_t run_batch(const Batch &b, const Layout &l, char *ws, cudaStream_t st
     // counts[nb] becomes the number of live (non-zero digit) entries
     ZK_TRY(scan(counts, nb + 1, cursor, counts));
     prof.mark("scan", stream);
-    if (scalars) {
-        scatter_kernel<<<grid_for(scalars, 256), 256, 0, stream>>>(b, cursor, reinterpret_cast<uint2 *>(sb));
+    for (u32 t = 0; t < b.ntasks; t++) {
+        const u64 first = b.sc_first[t], last = b.sc_first[t + 1];
+        if (last == first) continue;
+        scatter_kernel<<<grid_for(last - first, 256), 256, 0, stream>>>(b, cursor, reinterpret_cast<uint2 *>(sb),
+                                                                         first, last);
         ZK_TRY(cudaGetLastError());
     }
     prof.mark("scatter", stream);
