@@ -290,6 +290,8 @@ def run_gpu(args):
     # ---- poly library rows (evaluation, batched inversion, division by X - b)
     poly = measure_poly(zk, gen, dev, stream, hbm_peak=peaks()[0], mont_peak=mont_per_s) \
         if not args.no_fused else None
+    # ---- the pipelined fused kernel over host-resident polynomials
+    pipelined = measure_pipelined(zk, gen) if (not args.no_fused and rank == 0) else None
 
     # ---- batched form (mixed NTT/MSM workload) and served form (Poisson arrivals)
     batched = measure_batched(zk, args) if (not args.no_batched and rank == 0) else None
@@ -306,7 +308,7 @@ def run_gpu(args):
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_reference(args.ref_msm_log, args.ref_ntt_log)
     emit(args, zk, rank, world, n_msm, n_ntt, ntt_ms, msm_ms, step_ms, pass_ms, bitrev_ms, stage_ms, imad_per_s,
-         e2e_msm_s, e2e_ntt_s, cpu, clocks, bases, batched, served, fused, mont_per_s, poly)
+         e2e_msm_s, e2e_ntt_s, cpu, clocks, bases, batched, served, fused, mont_per_s, poly, pipelined)
 
 
 def measure_fused(zk, gen, dev, stream, hbm_peak, mont_peak, log_n=NTT_LOG, ext=3, reps=10):
@@ -341,6 +343,52 @@ def measure_fused(zk, gen, dev, stream, hbm_peak, mont_peak, log_n=NTT_LOG, ext=
     del a, b, c, z, q
     torch.cuda.empty_cache()
     return out
+
+
+def measure_pipelined(zk, gen, log_n=22, parts=8, reps=5):
+    """The pipelined fused kernel (host polynomials streamed through the device in chunks,
+    libzkp_pipeline.so) on the quotient-shaped graph over 2^log_n host-resident points: five
+    input polynomials and a periodic 1/Z_H in, one polynomial out, against the one-shot path
+    (copy everything in, one kernel, copy the result out).  Host clock (the call blocks)."""
+    import time
+    import torch
+    n = 1 << log_n
+    g = zk.fused.FusedGraph([
+        ("input", "a", "poly", "var", 0), ("input", "b", "poly", "var", 1), ("input", "c", "poly", "var", 2),
+        ("input", "z", "poly", "var", 3), ("input", "zw", "poly", "var", 4), ("input", "zh", "periodic", "var", 5),
+        ("mul", "ab", "a", "b"), ("sub", "t0", "ab", "c"), ("mul", "zz", "z", "zw"), ("sub", "t1", "t0", "zz"),
+        ("mul", "q", "t1", "zh"), ("output", 0, "q")])
+    op = zk.fused.FusedOp(g, "zkp_quotient_plain_inputs")
+    ins = [gen.fr(800 + i, n).cpu().pin_memory() for i in range(5)] + [gen.fr(805, 8).cpu().pin_memory()]
+    out = torch.empty((n, 8), dtype=torch.int32).pin_memory()
+    pk = zk.fused.PipelinedFusedKernel(op, parts)
+    kern = zk.fused.FusedKernel(op)
+    dev_in = [zk.ScalarArray(t.cuda()) for t in ins]
+    dev_out = zk.ScalarArray.zeros(n)
+
+    def one_shot():
+        for d, h in zip(dev_in, ins):
+            d.values.copy_(h, non_blocking=True)
+        kern([dev_out], dev_in)
+        out.copy_(dev_out.values, non_blocking=True)
+        torch.cuda.synchronize()
+
+    def timed(fn):
+        fn()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            fn()
+        return (time.perf_counter() - t0) / reps
+
+    t_pipe = timed(lambda: pk([out], ins, n))
+    t_one = timed(one_shot)
+    host_bytes = 5 * n * 32 + n * 32
+    return {"n": n, "parts": parts, "ms": t_pipe * 1e3, "elems_per_s": n / t_pipe,
+            "host_link_gbs": host_bytes / t_pipe / 1e9, "one_shot_ms": t_one * 1e3,
+            "speedup_vs_one_shot": t_one / t_pipe,
+            "device_bytes": pk.workspace.numel(), "one_shot_device_bytes": 6 * n * 32,
+            "note": "host-resident operands over PCIe; the chunked form needs 5 parts' worth of device "
+                    "buffers per operand set instead of the whole polynomials"}
 
 
 def measure_poly(zk, gen, dev, stream, hbm_peak, mont_peak, log_n=22, reps=10):
@@ -520,7 +568,7 @@ def run_e2e(zk, native, lib_msm, scalars, points, ntt_in, tw, stream, dev, local
 
 def emit(args, zk, rank, world, n_msm, n_ntt, ntt_ms, msm_ms, step_ms, pass_ms, bitrev_ms, stage_ms, imad_per_s,
          e2e_msm_s, e2e_ntt_s, cpu, clocks, bases, batched=None, served=None, fused=None, mont_per_s=None,
-         poly=None):
+         poly=None, pipelined=None):
     import torch
     if rank != 0:
         if world > 1:
@@ -610,6 +658,8 @@ def emit(args, zk, rank, world, n_msm, n_ntt, ntt_ms, msm_ms, step_ms, pass_ms, 
         line["fused"] = fused
     if poly:
         line["poly"] = poly
+    if pipelined:
+        line["fused_pipelined"] = pipelined
     if batched:
         line["batched"] = batched
     if served:

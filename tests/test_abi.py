@@ -14,12 +14,14 @@ HEADER_LIB = {
     "poly.h": "libpoly.so",
     "zkp_gen.h": "libzkp_gen.so",
     "zkp_runtime.h": "libzkp_runtime.so",
+    "zkp_pipeline.h": "libzkp_pipeline.so",
 }
 
 
 def declared_functions(header):
     text = open(os.path.join(ROOT, "include", header)).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    text = re.sub(r"\btypedef\b[^;]*;", "", text)  # function-pointer and struct typedefs
     return sorted(set(re.findall(r"\b(\w+)\s*\([^;{]*\)\s*;", text)) - {"if", "while", "for", "sizeof"})
 
 

@@ -126,3 +126,68 @@ def test_quotient_pipeline_config3_full(zk, orc):
     g = orc.to_mont(orc.int_to_limbs(7))
     ea, eb, ec = (orc.coset_ntt(orc.intt(x, k), k, k + ext, g) for x in (a, b, c))
     assert np.array_equal(got, quotient_oracle(orc, ea, eb, ec, z, zh_oracle(orc, k, ext), ext))
+
+
+def _host(a):
+    """(n, 4) uint64 limbs -> pinned (n, 8) int32 CPU tensor"""
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.uint64).view(np.int32).reshape(-1, 8).copy()).pin_memory()
+
+
+@pytest.mark.parametrize("parts", [4, 8, 16])
+def test_pipelined_fused_kernel(zk, orc, parts):
+    """The pipelined form (host polynomials streamed in chunks, fused_kernels.rs:198-516) gives
+    the one-shot kernel's results: a quotient-shaped graph with a periodic 1/Z_H input and an
+    in-out mutable polynomial (out = (a*b - c - z*zw) * zh + out)."""
+    n = 1 << 12
+    g = zk.fused.FusedGraph([
+        ("input", "a", "poly", "var", 0),
+        ("input", "b", "poly", "var", 1),
+        ("input", "c", "poly", "var", 2),
+        ("input", "z", "poly", "var", 3),
+        ("input", "zw", "poly", "var", 4),
+        ("input", "zh", "periodic", "var", 5),
+        ("input", "acc", "poly", "mut", 0),
+        ("mul", "ab", "a", "b"),
+        ("sub", "t0", "ab", "c"),
+        ("mul", "zz", "z", "zw"),
+        ("sub", "t1", "t0", "zz"),
+        ("mul", "q", "t1", "zh"),
+        ("add", "r", "q", "acc"),
+        ("output", 0, "r"),
+    ])
+    a, b, c, z, zw, acc = (orc.gen_fr(700 + i, n) for i in range(6))
+    zh = orc.gen_fr(706, 8)
+    t = orc.vec_sub(orc.vec_sub(orc.vec_mul(a, b), c), orc.vec_mul(z, zw))
+    expect = orc.vec_add(orc.vec_mul(t, np.tile(zh, (n // 8, 1))), acc)
+    op = zk.fused.FusedOp(g, "zkp_test_pipelined_q")
+    host_out = _host(acc)
+    zk.fused.PipelinedFusedKernel(op, parts)([host_out], [_host(x) for x in (a, b, c, z, zw, zh)], n)
+    assert np.array_equal(host_out.numpy().view(np.uint64).reshape(n, 4), expect)
+    # the one-shot kernel on device copies agrees
+    out = dev(zk, acc)
+    zk.fused.FusedKernel(op)([out], [dev(zk, x) for x in (a, b, c, z, zw, zh)])
+    assert np.array_equal(out.numpy_u64(), expect)
+
+
+def test_pipelined_fused_kernel_write_only_output(zk, orc):
+    """A mutable polynomial the kernel only writes is not copied in: stale host contents of
+    the output do not matter."""
+    n = 1 << 11
+    g = zk.fused.FusedGraph([("input", "a", "poly", "var", 0), ("input", "b", "poly", "var", 1),
+                             ("mul", "p", "a", "b"), ("sub", "d", "p", "a"), ("output", 0, "d")])
+    a, b = orc.gen_fr(720, n), orc.gen_fr(721, n)
+    out = _host(orc.gen_fr(722, n))  # stale contents
+    zk.fused.PipelinedFusedKernel(zk.fused.FusedOp(g, "zkp_test_pipelined_wo"), 8)([out], [_host(a), _host(b)], n)
+    assert np.array_equal(out.numpy().view(np.uint64).reshape(n, 4), orc.vec_sub(orc.vec_mul(a, b), a))
+
+
+def test_pipelined_fused_kernel_rejects_bad_split(zk, orc):
+    n = 1000
+    g = zk.fused.FusedGraph([("input", "a", "poly", "var", 0), ("input", "b", "poly", "var", 1),
+                             ("add", "s", "a", "b"), ("output", 0, "s")])
+    k = zk.fused.PipelinedFusedKernel(zk.fused.FusedOp(g, "zkp_test_pipelined_add"), 6)  # 6 does not divide 1000
+    a = orc.gen_fr(710, n)
+    with pytest.raises(ValueError):
+        k([_host(a)], [_host(a), _host(a)], n)
+    with pytest.raises(ValueError):
+        zk.fused.PipelinedFusedKernel(zk.fused.FusedOp(g, "zkp_test_pipelined_add"), 3)

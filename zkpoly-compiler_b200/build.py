@@ -24,6 +24,7 @@ LIBS = {
     "libmsm.so": ("msm.cu", ["-ldl"]),
     "libpoly.so": ("poly.cu", []),
     "libzkp_gen.so": ("gen.cu", []),
+    "libzkp_pipeline.so": ("pipeline.cu", []),
     # the served form links the kernel libraries above and finds them next to itself
     "libzkp_runtime.so": ("serve.cu", ["-L" + LIB, "-lntt", "-lmsm", "-lpoly", "-lzkp_gen", "-ldl", "-lpthread",
                                        "-Xlinker", "-rpath=$ORIGIN"]),

@@ -228,6 +228,53 @@ class FusedKernel:
                       stream_handle(stream)), self.op.name)
 
 
+class PipelinedFusedKernel:
+    """core/src/fused_kernels.rs:198-516: the same fused kernel over HOST polynomials, streamed
+    through the device in `divide_parts` chunks (> 3, dividing the length) with the copies of
+    consecutive chunks overlapping the kernel (libzkp_pipeline.so, include/zkp_pipeline.h).
+    For operands that do not fit device memory; results are identical to the one-shot kernel."""
+
+    def __init__(self, op: FusedOp, divide_parts: int = 4):
+        from .native import load
+        if divide_parts <= 3:
+            raise ValueError("divide_parts must be > 3 (fused_kernels.rs:201)")
+        self.kernel = FusedKernel(op)
+        self.divide_parts = divide_parts
+        self.lib = load("libzkp_pipeline.so")
+        self.workspace = None
+
+    @staticmethod
+    def _arg(t: torch.Tensor, stream_len: int, write_only: bool = False):
+        from .native import ZkpPipelineArg
+        if t.device.type != "cpu" or not t.is_contiguous() or t.dtype != torch.int32 or t.shape[-1] != 8:
+            raise ValueError("host arguments are contiguous (n, 8) int32 CPU tensors (pinned for overlap)")
+        rows = t.shape[0]
+        return ZkpPipelineArg(t.data_ptr(), 0 if rows == stream_len else rows, int(write_only))
+
+    def __call__(self, mut_vars: list, vars_: list, length: int) -> None:
+        """mut_vars / vars_: (rows, 8) int32 CPU tensors - polynomials of `length` rows, or
+        scalars / periodic inputs (fewer rows, copied once).  Blocks until the outputs are in
+        host memory."""
+        from .native import ZkpPipelineArg, check
+        g = self.kernel.op.graph
+        if len(vars_) != g.num_vars or len(mut_vars) != g.num_mut_vars:
+            raise ValueError("argument count differs from the graph's")
+        read_mut = {n[4] for n in g.nodes if n[0] == "input" and n[3] == "mut"}
+        va = (ZkpPipelineArg * max(len(vars_), 1))(*[self._arg(t, length) for t in vars_])
+        ma = (ZkpPipelineArg * max(len(mut_vars), 1))(*[self._arg(t, length, i not in read_mut)
+                                                          for i, t in enumerate(mut_vars)])
+        need = int(self.lib.zkp_fused_pipelined_workspace(va, len(vars_), ma, len(mut_vars), length,
+                                                          self.divide_parts))
+        if need == 0:
+            raise ValueError("invalid pipelined arguments (length % divide_parts, periodic lengths)")
+        if self.workspace is None or self.workspace.numel() < need:
+            self.workspace = torch.empty(need, dtype=torch.uint8, device="cuda")
+        fn = ctypes.cast(self.kernel.fn, ctypes.c_void_p).value
+        check(self.lib.zkp_fused_pipelined(fn, va, len(vars_), ma, len(mut_vars), length, self.divide_parts,
+                                           self.workspace.data_ptr(), self.workspace.numel(), None),
+              "zkp_fused_pipelined")
+
+
 # ------------------------------------------------------------------ graphs used by the path
 def quotient_graph() -> FusedGraph:
     """(a*b - c - z*z(wX)) * zh_inv[i mod 8] on the 8x extended coset: the quotient numerator

@@ -24,6 +24,12 @@ class PolyPtr(ctypes.Structure):
 
 ConstPolyPtr = PolyPtr  # identical layout (iter.cuh:20-26)
 
+
+class ZkpPipelineArg(ctypes.Structure):
+    """include/zkp_pipeline.h: a host polynomial streamed in chunks (whole = 0) or a host array
+    of `whole` elements copied once (scalars, periodic inputs)."""
+    _fields_ = [("host", ctypes.c_void_p), ("whole", ctypes.c_ulonglong), ("write_only", ctypes.c_uint)]
+
 _libs: dict[str, ctypes.CDLL] = {}
 
 # symbol -> (restype, argtypes)
@@ -72,6 +78,13 @@ SIGNATURES = {
                                                 ctypes.c_int]),
         "zkp_imad_probe": (cudaError_t, [ctypes.c_uint, ctypes.c_uint, c_void_p, c_void_p]),
         "zkp_mont_probe": (cudaError_t, [ctypes.c_uint, ctypes.c_uint, c_void_p, c_void_p]),
+    },
+    "libzkp_pipeline.so": {
+        "zkp_fused_pipelined_workspace": (ctypes.c_ulonglong, [c_void_p, ctypes.c_uint, c_void_p, ctypes.c_uint,
+                                                               ctypes.c_ulonglong, ctypes.c_ulonglong]),
+        "zkp_fused_pipelined": (cudaError_t, [c_void_p, c_void_p, ctypes.c_uint, c_void_p, ctypes.c_uint,
+                                              ctypes.c_ulonglong, ctypes.c_ulonglong, c_void_p, ctypes.c_ulonglong,
+                                              c_void_p]),
     },
     "libzkp_gen.so": {
         "zkp_gen_fr": (cudaError_t, [ctypes.c_ulonglong, ctypes.c_ulonglong, ctypes.c_ulonglong, c_void_p, c_void_p]),
