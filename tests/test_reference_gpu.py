@@ -101,6 +101,43 @@ def test_reference_ssip_ntt_matches(zk, log_n):
                           "speedup": ms_ref / ms}))
 
 
+@pytest.mark.parametrize("log_n", [4, 12, 17, 22])
+def test_reference_recompute_ntt_matches(zk, log_n):
+    """recompute_ntt (roots rebuilt from omegas and the pq table) and gen_pq_omegas against the
+    reference's own (recompute_ntt.cuh:362-438, precompute.cuh:89-113) on the same input; then
+    distribute_powers (distribute_powers.cuh:5-21) with a short powers array."""
+    ref = _ref_lib("libref_ntt.so")
+    ref.recompute_ntt.restype = ctypes.c_int
+    ref.recompute_ntt.argtypes = [zk.native.PolyPtr, ctypes.c_void_p, ctypes.c_uint, ctypes.c_void_p, ctypes.c_uint,
+                                  ctypes.c_void_p, ctypes.c_uint, ctypes.c_uint]
+    ref.gen_pq_omegas.restype = None
+    ref.gen_pq_omegas.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint, ctypes.c_uint, ctypes.c_void_p]
+    ref.distribute_powers.restype = ctypes.c_int
+    ref.distribute_powers.argtypes = [zk.native.PolyPtr, ctypes.c_void_p, ctypes.c_ulonglong, ctypes.c_void_p]
+    n = 1 << log_n
+    w = np.ascontiguousarray(zk.field.mont_words(zk.field.root_of_unity(log_n)), dtype=np.uint32).copy()
+    pq_len = zk.ntt.get_pq_len(log_n)
+    pq_deg = int(np.log2(pq_len)) + 1
+    pq, omegas = zk.ntt.gen_pq_omegas(pq_len, n, w)
+    pq_ref, om_ref = np.zeros_like(pq), np.zeros_like(omegas)
+    ref.gen_pq_omegas(pq_ref.ctypes.data, om_ref.ctypes.data, pq_deg, n, w.ctypes.data)
+    assert np.array_equal(pq, pq_ref) and np.array_equal(omegas, om_ref)
+    data = zk.gen.fr(350 + log_n, n)
+    x_ref, x = zk.ScalarArray(data.clone()), zk.ScalarArray(data.clone())
+    pq_d, om_d = zk.ScalarArray.from_numpy(pq), zk.ScalarArray.from_numpy(omegas)
+    st = torch.cuda.current_stream().cuda_stream
+    assert ref.recompute_ntt(x_ref.poly_ptr(), pq_d.values.data_ptr(), pq_deg, om_d.values.data_ptr(), log_n, st,
+                             8, 8) == 0
+    zk.ntt.recompute_ntt(x, pq_d, om_d)
+    torch.cuda.synchronize()
+    assert torch.equal(x_ref.values, x.values)
+    powers = zk.ScalarArray(zk.gen.fr(360, 7))
+    assert ref.distribute_powers(x_ref.poly_ptr(), powers.values.data_ptr(), 7, st) == 0
+    zk.ntt.distribute_powers(x, powers)
+    torch.cuda.synchronize()
+    assert torch.equal(x_ref.values, x.values)
+
+
 @pytest.mark.parametrize("log_n", [10, 16])
 def test_reference_msm_one_table_matches(zk, log_n):
     """The runtime's default library (window 16, 16 target windows: one table)."""
