@@ -12,12 +12,17 @@
 //                histograms.  With precomputed tables (reference MSMPrecompute,
 //                msm_impl.cuh:776-828) logical window j*Wp + w maps to table j, window w.
 //   2. scan:     exclusive prefix sum of the histograms gives every bucket's run.
-//   3. scatter:  digits are recomputed and each (point index, sign) lands in its bucket's run,
-//                so the array is sorted by (window, bucket) - a counting sort.
-//   4. accumulate: the sorted array is cut into equal chunks, one per thread; each thread
-//                walks its chunk with mixed additions.  Runs wholly inside a chunk are written
+//   3. scatter:  digits are recomputed and each (bucket id, point code = index | sign) record
+//                lands in its bucket's run, so the records are sorted by (window, bucket) - a
+//                counting sort (one launch per task of a batch).
+//   4a. pairing rounds (large MSMs): each round adds neighbouring points of every bucket's list
+//                in affine coordinates, all of a round's inverses from one inversion
+//                (Montgomery's trick over a CTA-level product tree), roughly halving the lists.
+//   4. accumulate: the (last) list is cut into equal chunks, one per thread; each thread walks
+//                its chunk with mixed XYZZ additions.  Runs wholly inside a chunk are written
 //                straight to their bucket; runs cut by a chunk boundary leave partial sums that
-//                a fix-up pass joins.  Load balance does not depend on the scalar distribution.
+//                a fix-up pass joins (one thread per recorded chain).  Load balance does not
+//                depend on the scalar distribution.
 //   5. reduce:   per window sum_b b * S_b: short segments form their sums and running sums
 //                (summation by parts), the segment sums are split by the bits of their
 //                index into classes summed in parallel, and the classes are scaled by
