@@ -209,6 +209,14 @@ struct Layout {
 inline size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
 
 
+// digit records and bucket ids are indexed with 32-bit positions: a batch must stay below 2^32 of
+// each (entry points refuse larger ones)
+inline bool batch_fits(const Batch &b) {
+    u64 entries = 0;
+    for (u32 t = 0; t < b.ntasks; t++) entries += b.task[t].n * b.task[t].W;
+    return entries < (1ull << 32) - 1 && b.key_first[b.ntasks] < (1ull << 32) - 1;
+}
+
 inline Layout make_layout(const Batch &b) {
     Layout l{};
     size_t off = 0;
@@ -1344,6 +1352,7 @@ extern "C" cudaError_t zkp_msm_device(void *workspace_d, unsigned long long work
     ZK_CHECK_ARG(c >= 2 && c <= 24 && nt >= 1);
     ZK_CHECK_ARG(n * nt < (1ull << 31));
     const msm::Batch b = msm::single(points_d, nt, scalars_d, n, c, result_d);
+    ZK_CHECK_ARG(msm::batch_fits(b));
     const msm::Layout l = msm::make_layout(b);
     ZK_CHECK_ARG(workspace_bytes >= l.total);
     return msm::run_batch(b, l, reinterpret_cast<char *>(workspace_d), stream);
@@ -1368,6 +1377,7 @@ static cudaError_t build_batch(const ZkpMsmTask *tasks, unsigned int ntasks, msm
         b.task[t].result = k.result_d;
     }
     msm::finish_batch(b);
+    ZK_CHECK_ARG(msm::batch_fits(b));
     *out = b;
     return cudaSuccess;
 }
@@ -1444,6 +1454,10 @@ extern "C" cudaError_t msm(void *const *buffers, unsigned long *buffer_sizes, un
     ZK_CHECK_ARG(num_cards >= 1 && cards != nullptr && len > 0);
     u32 c, nt;
     msm::resolve(len / num_cards + 1, 0, 0, &c, &nt);
+    {
+        const u64 per_card = len / num_cards + 1;  // 32-bit record positions and point codes
+        ZK_CHECK_ARG(per_card * ((msm::SCALAR_BITS + c - 1) / c) < (1ull << 32) - 1 && per_card * nt < (1ull << 31));
+    }
     // card k takes points [k*len/num_cards, (k+1)*len/num_cards)
     auto slice = [&](u32 k, u64 *lo, u64 *cnt) {
         *lo = len * k / num_cards;
@@ -1611,6 +1625,7 @@ extern "C" cudaError_t zkp_msm_device_noalloc(const unsigned int *points_d, unsi
     ZK_CHECK_ARG(n * nt < (1ull << 31));
     // no pairing rounds: their lists would not fit the fixed scratch
     const msm::Batch b = msm::single(points_d, nt, scalars_d, n, c, result_d, 0);
+    ZK_CHECK_ARG(msm::batch_fits(b));
     const msm::Layout l = msm::make_layout(b);
     // larger problems do not fit the fixed scratch: refuse instead of overrunning it
     if (l.total > kNoAllocScratchBytes) return cudaErrorInvalidValue;
