@@ -413,8 +413,33 @@ def measure_poly(zk, gen, dev, stream, hbm_peak, mont_peak, log_n=22, reps=10):
         ("batched_invert", lambda: zk.poly.batched_invert(inv, stream=stream), 64, 3),
         ("kate_division", lambda: zk.poly.kate_division(p, x, q, stream=stream), 64, 1),
     ]
+    # permute (lookup-argument permutation) over 2^20 rows, shaped like the reference's test
+    # (core/tests/poly.rs:569-625): table values uniform below 2n, inputs drawn from the table's
+    # distinct usable values, 25 unusable rows; small integers converted to Montgomery form
+    import numpy as np
+    m = 1 << 20
+    usable = m - 25
+    rng = np.random.default_rng(7)
+    tab = rng.integers(0, 2 * m, m, dtype=np.uint64)
+    distinct = np.unique(tab[:usable])
+    inp = distinct[rng.integers(0, len(distinct), m)]
+    r2 = zk.ScalarArray.from_numpy(np.array(zk.field.mont_words((1 << 256) % zk.field.FR_MODULUS),
+                                            dtype=np.uint32).reshape(1, 8))
+    lookup = []
+    for vals in (inp, tab):
+        limbs = np.zeros((m, 8), dtype=np.uint32)
+        limbs[:, 0] = vals.astype(np.uint32)
+        arr = zk.ScalarArray.from_numpy(limbs)
+        zk.ntt.distribute_powers(arr, r2)
+        lookup.append(arr)
+    ri, rt = zk.ScalarArray.alloc(usable), zk.ScalarArray.alloc(usable)
+    torch.cuda.synchronize()
     out = {"n": n}
-    for name, call, bpe, mpe in cases:
+    # permute: reads input and table (64 B a row), writes both outputs (64 B); no field products
+    # beyond the conversions in and out of Montgomery form
+    perm = ("permute", lambda: zk.poly.permute(lookup[0], lookup[1], usable, ri, rt, stream=stream), 128, 0)
+    for name, call, bpe, mpe in cases + [perm]:
+        rows = usable if name == "permute" else n
         for _ in range(2):
             call()
         torch.cuda.synchronize()
@@ -425,10 +450,11 @@ def measure_poly(zk, gen, dev, stream, hbm_peak, mont_peak, log_n=22, reps=10):
         e1.record(stream)
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / reps
-        out[name] = {"ms": ms, "elems_per_s": n / (ms / 1e3), "bytes_per_elem": bpe,
-                     "hbm_frac": bpe * n / (ms / 1e3) / 1e9 / hbm_peak, "fr_mults_per_elem": mpe,
-                     "mont_frac": mpe * n / (ms / 1e3) / mont_peak}
-    del p, inv, q
+        out[name] = {"ms": ms, "elems_per_s": rows / (ms / 1e3), "bytes_per_elem": bpe,
+                     "hbm_frac": bpe * rows / (ms / 1e3) / 1e9 / hbm_peak, "fr_mults_per_elem": mpe,
+                     "mont_frac": mpe * rows / (ms / 1e3) / mont_peak}
+    out["permute"]["rows"] = usable
+    del p, inv, q, lookup, ri, rt
     torch.cuda.empty_cache()
     return out
 
