@@ -193,6 +193,7 @@ def run_gpu(args):
         ntt_in = gen.fr(0, n_ntt, dev)
         x = zk.ScalarArray(ntt_in.clone())
         tw = zk.ntt.twiddle_table(NTT_LOG)
+        tw_shoup = zk.ntt.shoup_table(NTT_LOG)  # built once, like the root table
         if args.window:
             win, nt = args.window, args.tables or 1
         else:
@@ -207,6 +208,11 @@ def run_gpu(args):
     torch.cuda.synchronize()
 
     def ntt_step():
+        # the library's forward transform: register passes with the Shoup twiddle table
+        zk.ntt.ntt_ex(x, tw, stream=stream, shoup=tw_shoup)
+
+    def ssip_step():
+        # the reference-ABI entry (Montgomery root table only), timed separately below
         zk.ntt.ssip_ntt(x, tw, stream)
 
     def msm_step():
@@ -234,8 +240,17 @@ def run_gpu(args):
     ntt_ms = ev[0].elapsed_time(ev[1]) / args.steps
     msm_ms = ev[1].elapsed_time(ev[2]) / args.steps
     step_ms = ntt_ms + msm_ms
+    # the same transform through ssip_ntt (every rank runs it, outside the timed region)
+    for _ in range(2):
+        ssip_step()
+    ev[0].record(stream)
+    for _ in range(args.steps):
+        ssip_step()
+    ev[1].record(stream)
+    torch.cuda.synchronize()
+    ssip_ms = ev[0].elapsed_time(ev[1]) / args.steps
     if world > 1:
-        ntt_ms, msm_ms = max_over_ranks([ntt_ms, msm_ms], dev)
+        ntt_ms, msm_ms, ssip_ms = max_over_ranks([ntt_ms, msm_ms, ssip_ms], dev)
         step_ms = ntt_ms + msm_ms
 
     # ---- per-kernel timing from the libraries' own stream events (separate, untimed runs)
@@ -282,6 +297,16 @@ def run_gpu(args):
     e1.record(stream)
     torch.cuda.synchronize()
     mont_per_s = 5 * sms * 8 * 256 * mont_iters * 2 / (e0.elapsed_time(e1) / 1e3)
+    # ---- Shoup twiddle-product peak (the product of the NTT register passes)
+    lib_ntt = native.load("libntt.so")
+    lib_ntt.zkp_ntt_shoup_probe(sms * 8, mont_iters, mont_out.data_ptr(), stream.cuda_stream)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(5):
+        lib_ntt.zkp_ntt_shoup_probe(sms * 8, mont_iters, mont_out.data_ptr(), stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    shoup_per_s = 5 * sms * 8 * 256 * mont_iters * 2 / (e0.elapsed_time(e1) / 1e3)
 
     # ---- fused quotient kernel on the 2^24 extended coset (north_star's fused-kernel roofline)
     fused = measure_fused(zk, gen, dev, stream, hbm_peak=peaks()[0],
@@ -308,7 +333,8 @@ def run_gpu(args):
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_reference(args.ref_msm_log, args.ref_ntt_log)
     emit(args, zk, rank, world, n_msm, n_ntt, ntt_ms, msm_ms, step_ms, pass_ms, bitrev_ms, stage_ms, imad_per_s,
-         e2e_msm_s, e2e_ntt_s, cpu, clocks, bases, batched, served, fused, mont_per_s, poly, pipelined)
+         e2e_msm_s, e2e_ntt_s, cpu, clocks, bases, batched, served, fused, mont_per_s, poly, pipelined,
+         ssip_ms, shoup_per_s)
 
 
 def measure_fused(zk, gen, dev, stream, hbm_peak, mont_peak, log_n=NTT_LOG, ext=3, reps=10):
@@ -594,7 +620,7 @@ def run_e2e(zk, native, lib_msm, scalars, points, ntt_in, tw, stream, dev, local
 
 def emit(args, zk, rank, world, n_msm, n_ntt, ntt_ms, msm_ms, step_ms, pass_ms, bitrev_ms, stage_ms, imad_per_s,
          e2e_msm_s, e2e_ntt_s, cpu, clocks, bases, batched=None, served=None, fused=None, mont_per_s=None,
-         poly=None, pipelined=None):
+         poly=None, pipelined=None, ssip_ms=None, shoup_per_s=None):
     import torch
     if rank != 0:
         if world > 1:
@@ -647,14 +673,18 @@ def emit(args, zk, rank, world, n_msm, n_ntt, ntt_ms, msm_ms, step_ms, pass_ms, 
                 "ms": msm_ms, "stages_ms": stage_ms},
         "ntt": {"metric": f"NTT elems/s (2^{NTT_LOG})", "value": world * n_ntt / (ntt_ms / 1e3), "unit": "elems/s",
                 "ms": ntt_ms, "pass_ms": pass_avg, "bitrev_ms": statistics.median(bitrev_ms) if bitrev_ms else None,
-                "hbm_frac_whole_ntt": (64 * n_ntt / (ntt_ms / 1e3) / 1e9) / hbm_peak},
-        "roofline": {"kernel": f"ntt_pass_kernel (2^{max(digits)}-point sub-transform passes {digits} of the "
-                               f"2^{NTT_LOG} NTT)", "bound": "hbm",
+                "hbm_frac_whole_ntt": (64 * n_ntt / (ntt_ms / 1e3) / 1e9) / hbm_peak,
+                "path": "zkp_ntt_ex_shoup: register passes with Shoup twiddle products (root table + Shoup "
+                        "table of 64 B per root, both built once outside the timed region)",
+                "ssip_ms": ssip_ms, "ssip_value": world * n_ntt / (ssip_ms / 1e3) if ssip_ms else None,
+                "ssip_path": "ssip_ntt (reference ABI): the same passes with Montgomery twiddle products"},
+        "roofline": {"kernel": f"ntt_warp_pass_kernel (register passes of 2^d-point pencils, d = {digits}, "
+                               f"of the 2^{NTT_LOG} NTT; Shoup twiddle products)", "bound": "hbm",
                      "achieved": ntt_bytes_per_pass / (pass_avg / 1e3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
                      "frac": ntt_bytes_per_pass / (pass_avg / 1e3) / 1e9 / hbm_peak, "peak_source": peak_kind,
-                     # ncu DRAM bytes per pass launch: 58.7 B per element at 2^22 (four register
-                     # passes, 985 MB), scaled by the element count
-                     "traffic": 58.7 * n_ntt,
+                     # ncu DRAM bytes per pass launch: 68.3 B per element at 2^22 (four Shoup
+                     # register passes, 1146 MB), scaled by the element count
+                     "traffic": 68.3 * n_ntt,
                      "note": "IMAD-bound kernel: HBM fraction reported as asked; see int_roofline"},
         "int_roofline": {
             # denominator: Montgomery products per second of the library's own product routine
@@ -670,8 +700,13 @@ def emit(args, zk, rank, world, n_msm, n_ntt, ntt_ms, msm_ms, step_ms, pass_ms, 
                           "accounting": "160 n + 2 * 2^15 * 16 * 14 (c = 16 mixed-addition count), "
                                         "independent of the window and of the pairing rounds",
                           "frac": (msm_mults / (msm_total_ms / 1e3)) / mont_per_s},
+            # the register passes multiply by fixed twiddles with Shoup's product; their
+            # denominator is that product's own peak (zkp_ntt_shoup_probe, measured in this run)
+            "shoup_mul_peak_per_s": shoup_per_s,
             "ntt_passes": {"digits": digits, "fr_mults": ntt_mults, "ms": pass_avg * len(digits),
-                           "frac": (ntt_mults / (pass_avg * len(digits) / 1e3)) / mont_per_s},
+                           "fr_mults_per_s": ntt_mults / (pass_avg * len(digits) / 1e3),
+                           "frac": (ntt_mults / (pass_avg * len(digits) / 1e3)) / shoup_per_s,
+                           "peak": "shoup_mul_peak_per_s"},
         },
         "e2e": {"value": world * n_msm / e2e_msm_s if e2e_msm_s == e2e_msm_s else None, "unit": "points/s",
                 "h2d_bytes_per_step": n_msm * (64 + 32) + n_ntt * 32, "d2h_bytes_per_step": 64 + n_ntt * 32,

@@ -8,8 +8,9 @@
  * Errors come back as cudaError_t (cudaErrorInvalidValue for malformed arguments).
  *
  * The zkp_* symbols are additions with the same conventions (no counterpart in the
- * reference): fused inverse scaling, fused coset shift and a coset low-degree extension
- * that reads a shorter coefficient vector.
+ * reference): fused inverse scaling, fused coset shift, a coset low-degree extension
+ * that reads a shorter coefficient vector, and a second twiddle table format (Shoup pairs,
+ * 64 bytes per root) that makes the twiddle products of the register passes cheaper.
  */
 #ifndef ZKP_NTT_H
 #define ZKP_NTT_H
@@ -56,6 +57,25 @@ cudaError_t zkp_ntt_ex(PolyPtr x, const unsigned int *twiddle, unsigned int log_
 cudaError_t zkp_coset_lde(PolyPtr out, ConstPolyPtr in, const unsigned int *twiddle, unsigned int log_in,
                           unsigned int log_out, const unsigned int *shift_d, cudaStream_t stream);
 
+/* Twiddle table for Shoup's product by a fixed factor: entry e (16 words, 64 bytes) holds w^e
+ * as a plain value (8 words) and floor(w^e * 2^256 / r) (8 words), for e < 2^(log_len-1),
+ * built on the device from the Montgomery table twiddle_d ([w^0 .. w^(n/2-1)], as for
+ * ssip_ntt).  table_d: room for 2^(log_len-1) * 16 words.  Asynchronous, no allocation. */
+cudaError_t zkp_ntt_shoup_table(const unsigned int *twiddle_d, unsigned int log_len, unsigned int *table_d,
+                                cudaStream_t stream);
+
+/* zkp_ntt_ex and zkp_coset_lde whose register passes (the passes of at most 2^6-point pencils
+ * that make up the plan of every transform above 2^6 points) multiply by the twiddles of
+ * shoup_d, a zkp_ntt_shoup_table of the same twiddle table: 207 multiply instructions per
+ * twiddle product instead of the Montgomery product's 256, identical results.  twiddle is
+ * still read by the other passes; shoup_d = NULL gives zkp_ntt_ex / zkp_coset_lde. */
+cudaError_t zkp_ntt_ex_shoup(PolyPtr x, const unsigned int *twiddle, const unsigned int *shoup_d,
+                             unsigned int log_len, const unsigned int *shift_d, const unsigned int *scale_d,
+                             cudaStream_t stream);
+cudaError_t zkp_coset_lde_shoup(PolyPtr out, ConstPolyPtr in, const unsigned int *twiddle,
+                                const unsigned int *shoup_d, unsigned int log_in, unsigned int log_out,
+                                const unsigned int *shift_d, cudaStream_t stream);
+
 /* Device twin of ssip_precompute: out_d[i] = unit^i for i < count, unit_d on the device;
  * asynchronous on `stream`, no allocation. */
 cudaError_t zkp_ntt_roots_device(unsigned int *out_d, unsigned long long count, const unsigned int *unit_d,
@@ -94,6 +114,10 @@ typedef struct ZkpNttBatchPlan ZkpNttBatchPlan;
 cudaError_t zkp_ntt_batch_plan_create(const ZkpNttTask *tasks, unsigned int ntasks, ZkpNttBatchPlan **plan);
 cudaError_t zkp_ntt_batch_run(const ZkpNttBatchPlan *plan, cudaStream_t stream);
 void zkp_ntt_batch_plan_destroy(ZkpNttBatchPlan *plan);
+
+/* Benchmark support: throughput probe of the Shoup twiddle product (blocks x 256 threads x
+ * iters x 2 products; out_d holds blocks * 256 * 8 words). */
+cudaError_t zkp_ntt_shoup_probe(unsigned int blocks, unsigned int iters, unsigned int *out_d, cudaStream_t stream);
 
 /* Benchmark support: when enabled, the library records a CUDA event on the call's stream after
  * each launch of its next calls; read returns the per-launch milliseconds of the last call. */

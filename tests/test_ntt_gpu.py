@@ -213,3 +213,89 @@ def test_digit_caps_give_the_same_transform(zk, orc, log_n):
         assert lib.zkp_ntt_set_max_digit(log_n, 0) == 0
         zk.tuner.apply_ntt_plans()  # back to the tuned plan, if one is cached
     assert lib.zkp_ntt_set_max_digit(log_n, 3) != 0 and lib.zkp_ntt_set_max_digit(log_n, 13) != 0
+
+
+# ---- Shoup twiddle table and the register passes that read it
+def test_shoup_table_entries(zk, orc):
+    """Entry e = (w^e plain, floor(w^e 2^256 / r)) from the Montgomery root table."""
+    log_n = 12
+    p = zk.field.FR_MODULUS
+    tab = zk.ntt.shoup_table_of(zk.ntt.twiddle_table(log_n)).cpu().numpy().view(np.uint32)
+    w = zk.field.root_of_unity(log_n)
+    for e in (0, 1, 2, 777, (1 << (log_n - 1)) - 1):
+        we = pow(w, e, p)
+        got_w = orc.limbs_to_int(tab[e, :8].view(np.uint64))
+        got_ws = orc.limbs_to_int(tab[e, 8:].view(np.uint64))
+        assert got_w == we, e
+        assert got_ws == (we << 256) // p, e
+
+
+@pytest.mark.parametrize("log_n", [7, 8, 11, 12, 13, 17, 20, 22])
+def test_ntt_shoup_matches_best_fft(zk, orc, log_n):
+    """zkp_ntt_ex_shoup: bit-identical to the oracle's best_fft at sizes whose plans use register
+    passes of every width the tuner may pick."""
+    n = 1 << log_n
+    a = orc.gen_fr(90 + log_n, n)
+    x = to_dev(zk, a)
+    tw = zk.ntt.twiddle_table(log_n)
+    zk.ntt.ntt_ex(x, tw, shoup=zk.ntt.shoup_table_of(tw))
+    assert np.array_equal(x.numpy_u64(), orc.best_fft(a, orc.root_of_unity(log_n), log_n))
+
+
+@pytest.mark.parametrize("cap", [4, 5, 6])
+def test_ntt_shoup_every_pass_width(zk, orc, cap):
+    """Digit caps 4..6 route every pass of a 2^16 transform through the Shoup register pass with
+    that pencil width; the plan is restored afterwards."""
+    lib = zk.native.load("libntt.so")
+    log_n = 16
+    a = orc.gen_fr(123, 1 << log_n)
+    expect = orc.best_fft(a, orc.root_of_unity(log_n), log_n)
+    old = zk.ntt.plan_digits(log_n)
+    try:
+        assert lib.zkp_ntt_set_max_digit(log_n, cap) == 0
+        assert max(zk.ntt.plan_digits(log_n)) <= cap
+        x = to_dev(zk, a)
+        tw = zk.ntt.twiddle_table(log_n)
+        zk.ntt.ntt_ex(x, tw, shoup=zk.ntt.shoup_table_of(tw))
+        assert np.array_equal(x.numpy_u64(), expect)
+    finally:
+        assert lib.zkp_ntt_set_max_digit(log_n, max(old)) == 0
+
+
+def test_ntt_shoup_shift_scale_and_views(zk, orc):
+    """Shift and scale fused around Shoup passes, and a rotated view, equal the Montgomery path."""
+    log_n = 14
+    n = 1 << log_n
+    a = orc.gen_fr(131, n)
+    tw = zk.ntt.twiddle_table(log_n)
+    sh = zk.ntt.shoup_table_of(tw)
+    x1, x2 = to_dev(zk, a), to_dev(zk, a)
+    five, three = zk.ntt.scalar_const(5), zk.ntt.scalar_const(3)
+    zk.ntt.ntt_ex(x1, tw, shift=five, scale=three)
+    zk.ntt.ntt_ex(x2, tw, shift=five, scale=three, shoup=sh)
+    assert np.array_equal(x1.numpy_u64(), x2.numpy_u64())
+    base = to_dev(zk, a)
+    view = zk.ScalarArray(base.values, length=n, rotate=5)
+    ref = to_dev(zk, orc.poly_ptr_view(a, n, rotate=5))
+    zk.ntt.ntt_ex(view, tw, shoup=sh)
+    zk.ntt.ssip_ntt(ref, tw)
+    assert np.array_equal(view.numpy_u64(), ref.numpy_u64())
+
+
+def test_coset_lde_shoup_matches_oracle(zk, orc):
+    log_in, log_out = 12, 15
+    coef = orc.gen_fr(140, 1 << log_in)
+    g = orc.to_mont(orc.int_to_limbs(7))
+    tw = zk.ntt.twiddle_table(log_out)
+    out = zk.ScalarArray.zeros(1 << log_out)
+    zk.ntt.coset_lde(out, to_dev(zk, coef), tw, zk.ntt.scalar_const(7), shoup=zk.ntt.shoup_table_of(tw))
+    assert np.array_equal(out.numpy_u64(), orc.coset_ntt(coef, log_in, log_out, g))
+
+
+def test_shoup_entries_reject_misaligned_table(zk):
+    x = zk.ScalarArray.zeros(1 << 8)
+    tw = zk.ntt.twiddle_table(8)
+    sh = zk.ntt.shoup_table_of(tw)
+    lib = zk.native.load("libntt.so")
+    assert lib.zkp_ntt_ex_shoup(x.poly_ptr(), tw.values.data_ptr(), sh.data_ptr() + 4, 8, None, None, None) == 1
+    assert lib.zkp_ntt_shoup_table(tw.values.data_ptr(), 0, sh.data_ptr(), None) == 1

@@ -51,6 +51,7 @@ struct PassArgs {
     const u32 *omegas;      // [w^(2^i)] (recompute mode)
     const u32 *shift;       // coset shift (Montgomery) or null
     const u32 *scale;       // post-scale or null
+    const u32 *shoup;       // register passes: Shoup twiddle table (16 words per root) or null
     u32 L, D, lo, flags;
     u64 src_len;
 };
@@ -262,6 +263,9 @@ __global__ void __launch_bounds__(MAX_THREADS, 1) ntt_batch_pass_kernel(const Pa
 // group works on P pencils (1 or 2); with two, they differ only in their top index bits where
 // there are any, so both use the same twiddle and a twiddle load feeds two products.  No
 // shared memory and no block barrier; every element is one 32-byte sector in and out.
+// SH: the twiddle product is Shoup's (Fr::mul_shoup) from a table of (w^e plain,
+// floor(w^e 2^256 / m)) pairs, 64 bytes per root, built by shoup_table_kernel from the
+// Montgomery table; the results are the same values.
 constexpr u32 WARP_MAX_D = 6;
 
 ZK_DI void lane_swap(Fr &a, Fr &b, u32 lane, u32 k) {
@@ -272,7 +276,7 @@ ZK_DI void lane_swap(Fr &a, Fr &b, u32 lane, u32 k) {
     if (hi) a = send; else b = send;
 }
 
-template <u32 D, u32 P>
+template <u32 D, u32 P, bool SH>
 __global__ void __launch_bounds__(256) ntt_warp_pass_kernel(PassArgs a) {
     constexpr u32 g = 1u << (D - 1);  // lanes per pencil group
     const u32 lo = a.lo, L = a.L;
@@ -305,15 +309,23 @@ __global__ void __launch_bounds__(256) ntt_warp_pass_kernel(PassArgs a) {
         }
         const u64 low = (u64)(l & ((1u << k) - 1)) << lo;
         const u32 sh = L - 1 - lo - (u32)k;
-        Fr w;
+        Fr w, ws;
 #pragma unroll
         for (u32 j = 0; j < P; j++) {
             const u64 e = (low | c[j]) << sh;
             Fr s = Fr::add(x0[j], x1[j]);
             Fr d = Fr::sub(x0[j], x1[j]);
             if (e != 0) {
-                if (j == 0 || !shared_tw) w = Fr::load_nc(a.tw + e * 8);
-                d = Fr::mul(d, w);
+                if (SH) {
+                    if (j == 0 || !shared_tw) {
+                        w = Fr::load_nc(a.shoup + e * 16);
+                        ws = Fr::load_nc(a.shoup + e * 16 + 8);
+                    }
+                    d = Fr::mul_shoup(d, w, ws);
+                } else {
+                    if (j == 0 || !shared_tw) w = Fr::load_nc(a.tw + e * 8);
+                    d = Fr::mul(d, w);
+                }
             }
             x0[j] = s;
             x1[j] = d;
@@ -343,20 +355,35 @@ __global__ void __launch_bounds__(256) ntt_warp_pass_kernel(PassArgs a) {
 #define ZK_NTT_WARP_PENCILS 1  // pencils per lane group in the register pass (1 or 2)
 #endif
 
-template <u32 P>
+template <u32 P, bool SH>
 cudaError_t launch_warp_pass(const PassArgs &a, cudaStream_t stream) {
-    const u64 threads = 1ull << (a.L - 1 - (P == 2 ? 1 : 0));  // two elements of P pencils per thread
-    const u32 block = (u32)(threads < 256 ? threads : 256);
+    // two elements of P pencils per thread; CTAs of 128 threads: at 52 registers (the Shoup
+    // variant) 9 of them fit an SM, 36 warps, against 4 CTAs of 256 (32 warps), 5 % faster.
+    // The kernel keeps __launch_bounds__(256): with a bound of 128 the compiler takes 58
+    // registers and the occupancy gain is gone.
+    const u64 threads = 1ull << (a.L - 1 - (P == 2 ? 1 : 0));
+    const u32 block = (u32)(threads < 128 ? threads : 128);
     const u32 grid = (u32)(threads / block);
     switch (a.D) {
-        case 1: ntt_warp_pass_kernel<1, P><<<grid, block, 0, stream>>>(a); break;
-        case 2: ntt_warp_pass_kernel<2, P><<<grid, block, 0, stream>>>(a); break;
-        case 3: ntt_warp_pass_kernel<3, P><<<grid, block, 0, stream>>>(a); break;
-        case 4: ntt_warp_pass_kernel<4, P><<<grid, block, 0, stream>>>(a); break;
-        case 5: ntt_warp_pass_kernel<5, P><<<grid, block, 0, stream>>>(a); break;
-        default: ntt_warp_pass_kernel<6, P><<<grid, block, 0, stream>>>(a); break;
+        case 1: ntt_warp_pass_kernel<1, P, SH><<<grid, block, 0, stream>>>(a); break;
+        case 2: ntt_warp_pass_kernel<2, P, SH><<<grid, block, 0, stream>>>(a); break;
+        case 3: ntt_warp_pass_kernel<3, P, SH><<<grid, block, 0, stream>>>(a); break;
+        case 4: ntt_warp_pass_kernel<4, P, SH><<<grid, block, 0, stream>>>(a); break;
+        case 5: ntt_warp_pass_kernel<5, P, SH><<<grid, block, 0, stream>>>(a); break;
+        default: ntt_warp_pass_kernel<6, P, SH><<<grid, block, 0, stream>>>(a); break;
     }
     return cudaGetLastError();
+}
+
+// Shoup table entry e = (w^e plain, floor(w^e 2^256 / m)) from the Montgomery table entry e
+__global__ void __launch_bounds__(256) shoup_table_kernel(const u32 *tw, u64 count, u32 *out) {
+    const u64 stride = (u64)gridDim.x * blockDim.x;
+    for (u64 e = (u64)blockIdx.x * blockDim.x + threadIdx.x; e < count; e += stride) {
+        Fr w, ws;
+        Fr::mul_shoup_table_entry(Fr::load_nc(tw + e * 8), &w, &ws);
+        w.store(out + e * 16);
+        ws.store(out + e * 16 + 8);
+    }
 }
 
 // batched in-place bit reversal: element w of the concatenation belongs to task t
@@ -543,7 +570,10 @@ inline bool warp_pass_ok(const PassArgs &a) {
 }
 
 cudaError_t launch_pass(const PassArgs &a, cudaStream_t stream) {
-    if (warp_pass_ok(a)) return launch_warp_pass<ZK_NTT_WARP_PENCILS>(a, stream);
+    if (warp_pass_ok(a)) {
+        if (a.shoup) return launch_warp_pass<ZK_NTT_WARP_PENCILS, true>(a, stream);
+        return launch_warp_pass<ZK_NTT_WARP_PENCILS, false>(a, stream);
+    }
     ZK_TRY(ensure_smem_attr(ntt_pass_kernel, (int)pass_smem(MAX_D), g_attr_done));
     const u64 pencils = 1ull << (a.L - a.D);
     const u32 H = (1u << a.D) >> 1;
@@ -568,7 +598,7 @@ cudaError_t launch_pass(const PassArgs &a, cudaStream_t stream) {
 
 // Runs the full plan.  src (if non-null) is the pass-0 source for the coset LDE.
 cudaError_t run(const View &v, const View *src, u64 src_len, u32 L, const u32 *tw, const u32 *omegas,
-                const u32 *shift, const u32 *scale, cudaStream_t stream) {
+                const u32 *shift, const u32 *scale, cudaStream_t stream, const u32 *shoup = nullptr) {
     const Plan plan = make_plan(L, shift != nullptr || src != nullptr, omegas != nullptr);
     profiler().begin(stream);
     for (u32 p = 0; p < plan.np; p++) {
@@ -579,6 +609,7 @@ cudaError_t run(const View &v, const View *src, u64 src_len, u32 L, const u32 *t
         a.omegas = omegas;
         a.shift = shift;
         a.scale = scale;
+        a.shoup = shoup;
         a.L = L;
         a.D = plan.D[p];
         a.lo = plan.lo[p];
@@ -644,13 +675,78 @@ extern "C" cudaError_t zkp_ntt_ex(PolyPtr x, const unsigned int *twiddle, unsign
     return ntt::run(v, nullptr, 0, log_len, twiddle, nullptr, shift_d, scale_d, stream);
 }
 
+extern "C" cudaError_t zkp_ntt_ex_shoup(PolyPtr x, const unsigned int *twiddle, const unsigned int *shoup_d,
+                                        unsigned int log_len, const unsigned int *shift_d,
+                                        const unsigned int *scale_d, cudaStream_t stream) {
+    ZK_CHECK_ARG(log_len <= 28 && twiddle != nullptr);
+    ZK_CHECK_ARG(x.len == (1ull << log_len));
+    ZK_CHECK_ARG((reinterpret_cast<uintptr_t>(shoup_d) & 15) == 0);
+    View v;
+    ZK_CHECK_ARG(make_view(x, &v));
+    if (log_len == 0) {
+        if (!scale_d) return cudaSuccess;
+        return distribute_powers(x, scale_d, 1, stream);
+    }
+    return ntt::run(v, nullptr, 0, log_len, twiddle, nullptr, shift_d, scale_d, stream, shoup_d);
+}
+
 extern "C" cudaError_t zkp_coset_lde(PolyPtr out, ConstPolyPtr in, const unsigned int *twiddle, unsigned int log_in,
                                      unsigned int log_out, const unsigned int *shift_d, cudaStream_t stream) {
+    return zkp_coset_lde_shoup(out, in, twiddle, nullptr, log_in, log_out, shift_d, stream);
+}
+
+extern "C" cudaError_t zkp_coset_lde_shoup(PolyPtr out, ConstPolyPtr in, const unsigned int *twiddle,
+                                           const unsigned int *shoup_d, unsigned int log_in, unsigned int log_out,
+                                           const unsigned int *shift_d, cudaStream_t stream) {
     ZK_CHECK_ARG(log_out <= 28 && log_in <= log_out && log_out >= 1 && twiddle != nullptr);
     ZK_CHECK_ARG(out.len == (1ull << log_out) && in.len == (1ull << log_in));
+    ZK_CHECK_ARG((reinterpret_cast<uintptr_t>(shoup_d) & 15) == 0);
     View vo, vi;
     ZK_CHECK_ARG(make_view(out, &vo) && make_view(in, &vi));
-    return ntt::run(vo, &vi, in.len, log_out, twiddle, nullptr, shift_d, nullptr, stream);
+    return ntt::run(vo, &vi, in.len, log_out, twiddle, nullptr, shift_d, nullptr, stream, shoup_d);
+}
+
+// Shoup-product throughput probe (the twiddle product of the register passes): every thread
+// runs two independent chains of `iters` products x = x * w by fixed factors.
+__global__ void __launch_bounds__(256) shoup_probe_kernel(u32 iters, u32 *out) {
+    const u32 tid = blockIdx.x * blockDim.x + threadIdx.x;
+    Fr x, y, ys, u, v, vs;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        x.v[k] = (tid + 1) * 0x9e3779b9u + k * 0x85ebca6bu;
+        y.v[k] = (tid + 7) * 0xc2b2ae35u + k * 0x27d4eb2fu;
+        u.v[k] = x.v[k] ^ 0x165667b1u;
+        v.v[k] = y.v[k] ^ 0xd3a2646cu;
+        ys.v[k] = y.v[k] * 0x7feb352du;
+        vs.v[k] = v.v[k] * 0x846ca68bu;
+    }
+    x.v[7] &= 0x1fffffffu;  // below the modulus
+    y.v[7] &= 0x1fffffffu;
+    u.v[7] &= 0x1fffffffu;
+    v.v[7] &= 0x1fffffffu;
+    for (u32 i = 0; i < iters; i++) {
+        x = Fr::mul_shoup(x, y, ys);
+        u = Fr::mul_shoup(u, v, vs);
+    }
+    Fr::add(x, u).store(out + (u64)tid * 8);
+}
+
+// blocks x 256 threads x iters x 2 Shoup products; out_d holds blocks * 256 * 8 words
+extern "C" cudaError_t zkp_ntt_shoup_probe(unsigned int blocks, unsigned int iters, unsigned int *out_d,
+                                           cudaStream_t stream) {
+    shoup_probe_kernel<<<blocks, 256, 0, stream>>>(iters, out_d);
+    return cudaGetLastError();
+}
+
+extern "C" cudaError_t zkp_ntt_shoup_table(const unsigned int *twiddle_d, unsigned int log_len, unsigned int *table_d,
+                                           cudaStream_t stream) {
+    ZK_CHECK_ARG(log_len >= 1 && log_len <= 28 && twiddle_d != nullptr && table_d != nullptr);
+    ZK_CHECK_ARG((reinterpret_cast<uintptr_t>(twiddle_d) & 15) == 0 && (reinterpret_cast<uintptr_t>(table_d) & 15) == 0);
+    const u64 count = 1ull << (log_len - 1);
+    const u64 blocks = (count + 255) / 256;
+    const u32 grid = (u32)(blocks < (u64)num_sms() * 8 ? blocks : (u64)num_sms() * 8);
+    ntt::shoup_table_kernel<<<grid, 256, 0, stream>>>(twiddle_d, count, table_d);
+    return cudaGetLastError();
 }
 
 // ------------------------------------------------------------------ batched form

@@ -101,6 +101,8 @@ class Arena {
 struct SizeConsts {
     u32 *inv_tw = nullptr;   // inverse roots, 2^(k-1) entries
     u32 *fwd_tw = nullptr;   // forward roots of the extended size, 2^(k+ext-1) entries
+    u32 *inv_sh = nullptr;   // Shoup tables of the two (16 words per root)
+    u32 *fwd_sh = nullptr;
     u32 *ninv = nullptr;     // n^-1
     u32 *zh_inv = nullptr;   // 2^ext values of 1/Z_H on the coset
 };
@@ -227,11 +229,11 @@ cudaError_t launch_program(ZkpServer *s, Request *r, ZkpServer::Slot &slot) {
     RUN(zkp_gen_fr(seed + 3, 0, N, P(p.z), st));
     RUN(zkp_gen_fr(seed + 4, 0, 1, P(p.x), st));
     // three INTTs (n^-1 fused into the last pass)
-    RUN(zkp_ntt_ex(pp(P(p.a), n), sc.inv_tw, k, nullptr, sc.ninv, st));
-    RUN(zkp_ntt_ex(pp(P(p.b), n), sc.inv_tw, k, nullptr, sc.ninv, st));
-    RUN(zkp_ntt_ex(pp(P(p.c), n), sc.inv_tw, k, nullptr, sc.ninv, st));
+    RUN(zkp_ntt_ex_shoup(pp(P(p.a), n), sc.inv_tw, sc.inv_sh, k, nullptr, sc.ninv, st));
+    RUN(zkp_ntt_ex_shoup(pp(P(p.b), n), sc.inv_tw, sc.inv_sh, k, nullptr, sc.ninv, st));
+    RUN(zkp_ntt_ex_shoup(pp(P(p.c), n), sc.inv_tw, sc.inv_sh, k, nullptr, sc.ninv, st));
     // coset NTT of c on the extended domain
-    RUN(zkp_coset_lde(pp(P(p.e), N), cp(P(p.c), n), sc.fwd_tw, k, k + ext, s->shift, st));
+    RUN(zkp_coset_lde_shoup(pp(P(p.e), N), cp(P(p.c), n), sc.fwd_tw, sc.fwd_sh, k, k + ext, s->shift, st));
     // fused quotient: vars = [e, e, e, z, z(wX), zh_inv], mut = [q]
     PolyPtr *stage = reinterpret_cast<PolyPtr *>(slot.host + 96);
     stage[0] = pp(P(p.e), N);
@@ -411,6 +413,8 @@ extern "C" cudaError_t zkp_serve_create(const ZkpServeConfig *cfg, const unsigne
         const u64 n = 1ull << k;
         e = cudaMalloc(&c.inv_tw, (n / 2) * 32);
         if (e == cudaSuccess) e = cudaMalloc(&c.fwd_tw, (n << ext) / 2 * 32);
+        if (e == cudaSuccess) e = cudaMalloc(&c.inv_sh, (n / 2) * 64);
+        if (e == cudaSuccess) e = cudaMalloc(&c.fwd_sh, (n << ext) / 2 * 64);
         if (e == cudaSuccess) e = cudaMalloc(&c.ninv, 32);
         if (e == cudaSuccess) e = cudaMalloc(&c.zh_inv, (32u << ext));
         if (e != cudaSuccess) break;
@@ -421,6 +425,8 @@ extern "C" cudaError_t zkp_serve_create(const ZkpServeConfig *cfg, const unsigne
         zkh::Fe wf = zkh::fr_root_of_unity(k + ext, false);
         if (e == cudaSuccess) e = cudaMemcpy(tmp, wf.l, 32, cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = zkp_ntt_roots_device(c.fwd_tw, (n << ext) / 2, tmp, 0);
+        if (e == cudaSuccess) e = zkp_ntt_shoup_table(c.inv_tw, k, c.inv_sh, 0);
+        if (e == cudaSuccess) e = zkp_ntt_shoup_table(c.fwd_tw, k + ext, c.fwd_sh, 0);
         if (e == cudaSuccess) e = cudaDeviceSynchronize();
         zkh::Fe ninv = zkh::inv(F, zkh::from_u64(F, n));
         if (e == cudaSuccess) e = cudaMemcpy(c.ninv, ninv.l, 32, cudaMemcpyHostToDevice);
@@ -527,6 +533,8 @@ extern "C" void zkp_serve_destroy(ZkpServer *s) {
     for (auto &c : s->consts) {
         cudaFree(c.inv_tw);
         cudaFree(c.fwd_tw);
+        cudaFree(c.inv_sh);
+        cudaFree(c.fwd_sh);
         cudaFree(c.ninv);
         cudaFree(c.zh_inv);
     }

@@ -44,6 +44,11 @@ SIGNATURES = {
         "zkp_ntt_ex": (cudaError_t, [PolyPtr, c_void_p, ctypes.c_uint, c_void_p, c_void_p, c_void_p]),
         "zkp_coset_lde": (cudaError_t, [PolyPtr, PolyPtr, c_void_p, ctypes.c_uint, ctypes.c_uint, c_void_p,
                                         c_void_p]),
+        "zkp_ntt_shoup_table": (cudaError_t, [c_void_p, ctypes.c_uint, c_void_p, c_void_p]),
+        "zkp_ntt_shoup_probe": (cudaError_t, [ctypes.c_uint, ctypes.c_uint, c_void_p, c_void_p]),
+        "zkp_ntt_ex_shoup": (cudaError_t, [PolyPtr, c_void_p, c_void_p, ctypes.c_uint, c_void_p, c_void_p, c_void_p]),
+        "zkp_coset_lde_shoup": (cudaError_t, [PolyPtr, PolyPtr, c_void_p, c_void_p, ctypes.c_uint, ctypes.c_uint,
+                                              c_void_p, c_void_p]),
         "zkp_ntt_num_passes": (ctypes.c_uint, [ctypes.c_uint]),
         "zkp_ntt_plan_digits": (ctypes.c_uint, [ctypes.c_uint, c_void_p, ctypes.c_uint]),
         "zkp_ntt_set_max_digit": (cudaError_t, [ctypes.c_uint, ctypes.c_uint]),

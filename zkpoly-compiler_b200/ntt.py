@@ -99,16 +99,36 @@ def get_pq_len(log_len: int, stage_threads=(8, 8)) -> int:
 
 
 def ntt_ex(x: ScalarArray, twiddle: ScalarArray, shift: torch.Tensor | None = None,
-           scale: torch.Tensor | None = None, stream=None) -> None:
+           scale: torch.Tensor | None = None, stream=None, shoup: torch.Tensor | None = None) -> None:
+    """zkp_ntt_ex; with `shoup` (shoup_table_of(twiddle)) the register passes use Shoup's product."""
     log_len = _log2_exact(x.len)
-    check(_lib().zkp_ntt_ex(x.poly_ptr(), twiddle.values.data_ptr(), log_len, _ptr(shift), _ptr(scale),
-                            stream_handle(stream)), "zkp_ntt_ex")
+    if shoup is None:
+        check(_lib().zkp_ntt_ex(x.poly_ptr(), twiddle.values.data_ptr(), log_len, _ptr(shift), _ptr(scale),
+                                stream_handle(stream)), "zkp_ntt_ex")
+    else:
+        check(_lib().zkp_ntt_ex_shoup(x.poly_ptr(), twiddle.values.data_ptr(), shoup.data_ptr(), log_len,
+                                      _ptr(shift), _ptr(scale), stream_handle(stream)), "zkp_ntt_ex_shoup")
 
 
 def coset_lde(out: ScalarArray, inp: ScalarArray, twiddle: ScalarArray, shift: torch.Tensor,
-              stream=None) -> None:
-    check(_lib().zkp_coset_lde(out.poly_ptr(), inp.poly_ptr(), twiddle.values.data_ptr(), _log2_exact(inp.len),
-                               _log2_exact(out.len), _ptr(shift), stream_handle(stream)), "zkp_coset_lde")
+              stream=None, shoup: torch.Tensor | None = None) -> None:
+    if shoup is None:
+        check(_lib().zkp_coset_lde(out.poly_ptr(), inp.poly_ptr(), twiddle.values.data_ptr(),
+                                   _log2_exact(inp.len), _log2_exact(out.len), _ptr(shift), stream_handle(stream)),
+              "zkp_coset_lde")
+    else:
+        check(_lib().zkp_coset_lde_shoup(out.poly_ptr(), inp.poly_ptr(), twiddle.values.data_ptr(),
+                                         shoup.data_ptr(), _log2_exact(inp.len), _log2_exact(out.len), _ptr(shift),
+                                         stream_handle(stream)), "zkp_coset_lde_shoup")
+
+
+def shoup_table_of(twiddle: ScalarArray, stream=None) -> torch.Tensor:
+    """Shoup twiddle table (16 words per root: the plain root and floor(root * 2^256 / r)) built on
+    the device from the Montgomery table `twiddle` of a size-2 * twiddle.len transform."""
+    out = torch.empty((twiddle.len, 16), dtype=torch.int32, device=twiddle.values.device)
+    check(_lib().zkp_ntt_shoup_table(twiddle.values.data_ptr(), _log2_exact(twiddle.len) + 1, out.data_ptr(),
+                                     stream_handle(stream)), "zkp_ntt_shoup_table")
+    return out
 
 
 def plan_digits(log_len: int) -> list[int]:
@@ -139,27 +159,41 @@ def scalar_const(value: int, device: str = "cuda") -> torch.Tensor:
     return device_words(field.mont_words(value)[None, :], device)
 
 
+@functools.lru_cache(maxsize=64)
+def shoup_table(log_n: int, inverse: bool = False, device: str = "cuda") -> torch.Tensor:
+    """Shoup table of twiddle_table(log_n, inverse), for the library's own transforms."""
+    tab = shoup_table_of(twiddle_table(log_n, inverse, device))
+    torch.cuda.current_stream().synchronize()
+    return tab
+
+
 def n_inv(log_n: int, device: str = "cuda") -> torch.Tensor:
     return scalar_const(pow(1 << log_n, -1, field.FR_MODULUS), device)
 
 
 # ------------------------------------------------------------------ compiler-level compositions
 def ntt(x: ScalarArray, stream=None) -> None:
-    """Forward NTT at the natural root of the size (NTT(w))."""
-    ssip_ntt(x, twiddle_table(_log2_exact(x.len), False), stream)
+    """Forward NTT at the natural root of the size (NTT(w)); the register passes multiply by the
+    Shoup table of the root table (same values as ssip_ntt with the root table alone)."""
+    log_n = _log2_exact(x.len)
+    if log_n == 0:
+        return
+    ntt_ex(x, twiddle_table(log_n, False), stream=stream, shoup=shoup_table(log_n, False))
 
 
 def intt(x: ScalarArray, stream=None) -> None:
     """INTT = NTT(w^-1) then * n^-1 (intt_mending.rs:11-70), the scale fused into the last pass."""
     log_n = _log2_exact(x.len)
-    ntt_ex(x, twiddle_table(log_n, True), None, n_inv(log_n), stream)
+    ntt_ex(x, twiddle_table(log_n, True), None, n_inv(log_n), stream,
+           shoup=shoup_table(log_n, True) if log_n >= 1 else None)
 
 
 def coset_ntt(out: ScalarArray, coef: ScalarArray, shift: int = field.GENERATOR, stream=None) -> None:
     """Evaluations of the coefficient vector `coef` on shift * <w_out>: zero-extend,
     multiply by shift^i, NTT at the extended size, all fused (poly_coef.rs:252-255 Extend +
     distribute_powers.cuh:5-21 + NTT)."""
-    coset_lde(out, coef, twiddle_table(_log2_exact(out.len), False), scalar_const(shift), stream)
+    log_n = _log2_exact(out.len)
+    coset_lde(out, coef, twiddle_table(log_n, False), scalar_const(shift), stream, shoup=shoup_table(log_n, False))
 
 
 # ------------------------------------------------------------------ batched form
