@@ -120,20 +120,25 @@ def tune_msm(log_ns=range(12, 23), candidates=range(8, 21), bases=None) -> dict:
     return out
 
 
-def tune_ntt(log_ns=range(14, 25), candidates=(8, 9, 10, 11, 12), apply: bool = True) -> dict:
+def tune_ntt(log_ns=range(14, 25), candidates=(8, 9, 10, 11, 12), apply: bool = True, path: str = "shoup") -> dict:
     """Times a forward NTT of 2^L seeded elements for each digit cap (zkp_ntt_set_max_digit)
-    and caches the fastest per size; with apply the winners are set in the library."""
+    and caches the fastest per size; with apply the winners are set in the library.  path
+    "shoup" times the library's own transform (ntt.ntt: register passes with the Shoup twiddle
+    table), "ssip" the reference-ABI ssip_ntt (Montgomery twiddle products); the caps are shared
+    by both."""
     from . import gen, ntt
     from .scalar import ScalarArray
+    assert path in ("shoup", "ssip")
     lib = load(ntt.LIB)
     out, times = {}, {}
     for L in log_ns:
         x = ScalarArray(gen.fr(79, 1 << L))
         tw = ntt.twiddle_table(L)
+        run = (lambda: ntt.ntt(x)) if path == "shoup" else (lambda: ntt.ssip_ntt(x, tw))
         best = None
         for d in candidates:
             check(lib.zkp_ntt_set_max_digit(L, d), "zkp_ntt_set_max_digit")
-            t = _time(lambda: ntt.ssip_ntt(x, tw), reps=3)
+            t = _time(run, reps=10 if L < 20 else 3)
             times[f"{L}:{d}"] = t
             if best is None or t < best[1]:
                 best = (d, t)
