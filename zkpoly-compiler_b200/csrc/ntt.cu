@@ -663,16 +663,7 @@ extern "C" cudaError_t ssip_ntt(PolyPtr x, const unsigned int *twiddle, unsigned
 
 extern "C" cudaError_t zkp_ntt_ex(PolyPtr x, const unsigned int *twiddle, unsigned int log_len,
                                   const unsigned int *shift_d, const unsigned int *scale_d, cudaStream_t stream) {
-    ZK_CHECK_ARG(log_len <= 28 && twiddle != nullptr);
-    ZK_CHECK_ARG(x.len == (1ull << log_len));
-    View v;
-    ZK_CHECK_ARG(make_view(x, &v));
-    if (log_len == 0) {
-        // a length-1 transform is the identity, but shift^0 = 1 and the scale still apply
-        if (!scale_d) return cudaSuccess;
-        return distribute_powers(x, scale_d, 1, stream);
-    }
-    return ntt::run(v, nullptr, 0, log_len, twiddle, nullptr, shift_d, scale_d, stream);
+    return zkp_ntt_ex_shoup(x, twiddle, nullptr, log_len, shift_d, scale_d, stream);
 }
 
 extern "C" cudaError_t zkp_ntt_ex_shoup(PolyPtr x, const unsigned int *twiddle, const unsigned int *shoup_d,
@@ -684,6 +675,7 @@ extern "C" cudaError_t zkp_ntt_ex_shoup(PolyPtr x, const unsigned int *twiddle, 
     View v;
     ZK_CHECK_ARG(make_view(x, &v));
     if (log_len == 0) {
+        // a length-1 transform is the identity, but shift^0 = 1 and the scale still apply
         if (!scale_d) return cudaSuccess;
         return distribute_powers(x, scale_d, 1, stream);
     }
