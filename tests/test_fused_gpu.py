@@ -191,3 +191,44 @@ def test_pipelined_fused_kernel_rejects_bad_split(zk, orc):
         k([_host(a)], [_host(a), _host(a)], n)
     with pytest.raises(ValueError):
         zk.fused.PipelinedFusedKernel(zk.fused.FusedOp(g, "zkp_test_pipelined_add"), 3)
+
+
+def test_fixed_factor_products(zk, orc):
+    """Products with a scalar or periodic operand (either side) take Shoup's product from
+    per-CTA pairs; a periodic input above the shared-memory cap falls back to the Montgomery
+    product.  Results are identical to the oracle's."""
+    n = 4096
+    a = orc.gen_fr(20, n)
+    s = orc.gen_fr(21, 1)[0]
+    p8 = orc.gen_fr(22, 8)
+    p128 = orc.gen_fr(23, 128)
+    g = zk.fused.FusedGraph([
+        ("input", "a", "poly", "var", 0),
+        ("input", "s", "scalar", "var", 1),
+        ("input", "p", "periodic", "var", 2),
+        ("input", "q", "periodic", "var", 3),
+        ("mul", "as_", "a", "s"),
+        ("mul", "sa", "s", "a"),
+        ("mul", "ap", "a", "p"),
+        ("mul", "pa", "p", "a"),
+        ("mul", "aq", "a", "q"),
+        ("add", "u", "as_", "s"),        # s also read as a plain value
+        ("mul", "v", "u", "pa"),
+        ("sub", "w", "ap", "p"),         # p also read as a plain value
+        ("output", 0, "sa"),
+        ("output", 1, "v"),
+        ("output", 2, "w"),
+        ("output", 3, "aq"),
+    ])
+    kern = zk.fused.FusedKernel(zk.fused.FusedOp(g))
+    outs = [zk.ScalarArray.zeros(n) for _ in range(4)]
+    kern(outs, [dev(zk, a), scal(zk, s), dev(zk, p8), dev(zk, p128)])
+    pf = np.tile(p8, (n // 8, 1))
+    qf = np.tile(p128, (n // 128, 1))
+    sv = np.tile(s, (n, 1))
+    as_ = orc.vec_mul(a, sv)
+    pa = orc.vec_mul(pf, a)
+    exp = [orc.vec_mul(sv, a), orc.vec_mul(orc.vec_add(as_, sv), pa), orc.vec_sub(orc.vec_mul(a, pf), pf),
+           orc.vec_mul(a, qf)]
+    for o, e in zip(outs, exp):
+        assert np.array_equal(o.numpy_u64(), e)

@@ -38,10 +38,27 @@ ZK_DI View device_view(const ConstPolyPtr &p) {
     return device_view(q);
 }
 
-// element i of a periodic input (length divides the kernel length)
-ZK_DI u32 *periodic_at(const View &v, u64 i) {
-    const u64 k = (v.len & (v.len - 1)) == 0 ? (i & (v.len - 1)) : (i % v.len);
-    return v.at(k);
+// index into a periodic input for element i (its length divides the kernel length)
+ZK_DI u64 periodic_index(const View &v, u64 i) {
+    return (v.len & (v.len - 1)) == 0 ? (i & (v.len - 1)) : (i % v.len);
+}
+
+// element i of a periodic input
+ZK_DI u32 *periodic_at(const View &v, u64 i) { return v.at(periodic_index(v, i)); }
+
+// Products by a fixed factor (a scalar input, or a periodic input of at most SHOUP_PERIOD_MAX
+// entries) use Fr::mul_shoup: each CTA turns the factor's values into (w, ws) pairs in shared
+// memory once, 16 words per value, and every element's product reads them from there.
+constexpr u32 SHOUP_PERIOD_MAX = 64;
+
+// pairs for `count` Montgomery values at v[0..count) into sm (16 words each); the caller syncs
+ZK_DI void shoup_pairs(const View &v, u64 count, u32 *sm) {
+    for (u64 k = threadIdx.x; k < count; k += blockDim.x) {
+        Fr w, ws;
+        Fr::mul_shoup_table_entry(Fr::load(v.at(k)), &w, &ws);
+        w.store(sm + k * 16);
+        ws.store(sm + k * 16 + 8);
+    }
 }
 
 inline u32 fused_grid(u64 len, u32 block) {

@@ -75,22 +75,68 @@ class FusedOp:
     def get_temp_buffer_size(self) -> int:
         return 0
 
+    def _shoup_factors(self) -> dict:
+        """mul node name -> (factor input, other operand) for products with exactly one operand
+        that is a scalar or periodic input: those use Shoup's product by a fixed factor."""
+        inputs = {n[1]: n[2] for n in self.graph.nodes if n[0] == "input"}
+        fixed = {k for k, kind in inputs.items() if kind in ("scalar", "periodic")}
+        out = {}
+        for n in self.graph.nodes:
+            if n[0] == "mul":
+                _, name, lhs, rhs = n
+                if (rhs in fixed) != (lhs in fixed):
+                    out[name] = (rhs, lhs) if rhs in fixed else (lhs, rhs)
+        return out
+
     def gen_source(self) -> str:
         g = self.graph
         kinds = {}
-        pre, body = [], []
+        pre, setup, body = [], [], []
+        shoup = self._shoup_factors()
+        factors = {f for f, _ in shoup.values()}
+        # inputs read as plain values somewhere (not only as a Shoup factor)
+        plain_uses = set()
+        for n in g.nodes:
+            if n[0] == "output":
+                plain_uses.add(n[2])
+            elif n[0] != "input" and not (n[0] == "mul" and n[1] in shoup):
+                plain_uses.update(x for x in n[2:] if isinstance(x, str))
+            elif n[0] == "mul":
+                plain_uses.add(shoup[n[1]][1])
+        where = {}
         for n in g.nodes:
             op = n[0]
             if op == "input":
                 _, name, kind, side, idx = n
                 arr = "sv" if side == "var" else "smv"
+                where[name] = f"{arr}[{idx}]"
                 kinds[name] = kind
                 if kind == "scalar":
-                    pre.append(f"    const Fr {name} = Fr::load({arr}[{idx}].base);")
+                    if name in plain_uses:
+                        pre.append(f"    const Fr {name} = Fr::load({arr}[{idx}].base);")
+                    if name in factors:
+                        setup.append(f"    __shared__ __align__(16) u32 shs_{name}[16];")
+                        setup.append(f"    if (threadIdx.x == 0) fused::shoup_pairs({arr}[{idx}], 1, shs_{name});")
                 elif kind == "periodic":
-                    body.append(f"        const Fr {name} = Fr::load(fused::periodic_at({arr}[{idx}], idx));")
+                    body.append(f"        const u64 {name}_k = fused::periodic_index({arr}[{idx}], idx);")
+                    if name in plain_uses:
+                        body.append(f"        const Fr {name} = Fr::load({arr}[{idx}].at({name}_k));")
+                    if name in factors:
+                        setup.append(f"    __shared__ __align__(16) u32 shp_{name}[fused::SHOUP_PERIOD_MAX * 16];")
+                        setup.append(f"    const bool {name}_fx = {arr}[{idx}].len <= fused::SHOUP_PERIOD_MAX;")
+                        setup.append(f"    if ({name}_fx) fused::shoup_pairs({arr}[{idx}], {arr}[{idx}].len, shp_{name});")
                 else:
                     body.append(f"        const Fr {name} = Fr::load({arr}[{idx}].at(idx));")
+            elif op == "mul" and n[1] in shoup:
+                _, name, lhs, rhs = n
+                f, o = shoup[name]
+                if kinds[f] == "scalar":
+                    body.append(f"        const Fr {name} = Fr::mul_shoup({o}, Fr::load(shs_{f}), "
+                                f"Fr::load(shs_{f} + 8));")
+                else:
+                    body.append(f"        const Fr {name} = {f}_fx ? Fr::mul_shoup({o}, Fr::load(shp_{f} + {f}_k * 16), "
+                                f"Fr::load(shp_{f} + {f}_k * 16 + 8)) : Fr::mul({o}, Fr::load({where[f]}.at({f}_k)));")
+                kinds[name] = "scalar" if kinds[lhs] == kinds[rhs] == "scalar" else "poly"
             elif op in _BIN:
                 _, name, lhs, rhs = n
                 body.append(f"        const Fr {name} = {_BIN[op]}({lhs}, {rhs});")
@@ -134,6 +180,8 @@ __global__ void __launch_bounds__(256) {self.name}_kernel(const ConstPolyPtr *va
     if (threadIdx.x < {g.num_vars}) sv[threadIdx.x] = fused::device_view(vars[threadIdx.x]);
     if (threadIdx.x < {g.num_mut_vars}) smv[threadIdx.x] = fused::device_view(mut_vars[threadIdx.x]);
     __syncthreads();
+{chr(10).join(setup)}
+{"    __syncthreads();" if setup else ""}
 {chr(10).join(pre)}
     const u64 stride = (u64)gridDim.x * blockDim.x;
     for (u64 idx = (u64)blockIdx.x * blockDim.x + threadIdx.x; idx < len; idx += stride) {{
