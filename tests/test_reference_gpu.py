@@ -78,12 +78,14 @@ def test_reference_ssip_ntt_matches(zk, log_n):
     n = 1 << log_n
     data = zk.gen.fr(300 + log_n, n)
     tw = zk.ntt.twiddle_table(log_n)
-    x_ref, x = zk.ScalarArray(data.clone()), zk.ScalarArray(data.clone())
+    x_ref, x, x_sh = (zk.ScalarArray(data.clone()) for _ in range(3))
     stream = torch.cuda.current_stream().cuda_stream
     assert ref.ssip_ntt(x_ref.poly_ptr(), tw.values.data_ptr(), log_n, stream, 8, 8) == 0
     zk.ntt.ssip_ntt(x, tw)
+    zk.ntt.ntt(x_sh)  # the library's own transform (Shoup twiddle table)
     torch.cuda.synchronize()
     assert torch.equal(x_ref.values, x.values)
+    assert torch.equal(x_ref.values, x_sh.values)
     if TIMING and log_n >= 20:
         def t(fn, reps=5):
             fn()
@@ -97,8 +99,9 @@ def test_reference_ssip_ntt_matches(zk, log_n):
             return e0.elapsed_time(e1) / reps
         ms_ref = t(lambda: ref.ssip_ntt(x_ref.poly_ptr(), tw.values.data_ptr(), log_n, stream, 8, 8))
         ms = t(lambda: zk.ntt.ssip_ntt(x, tw))
+        ms_sh = t(lambda: zk.ntt.ntt(x_sh))
         print(json.dumps({"compare": "ssip_ntt", "log_n": log_n, "reference_ms": ms_ref, "this_ms": ms,
-                          "speedup": ms_ref / ms}))
+                          "speedup": ms_ref / ms, "this_shoup_ms": ms_sh, "speedup_shoup": ms_ref / ms_sh}))
 
 
 @pytest.mark.parametrize("log_n", [4, 12, 17, 22])
