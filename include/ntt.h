@@ -97,21 +97,28 @@ unsigned int zkp_ntt_num_passes(unsigned int log_len);
 
 /* ---- batched form (no counterpart in the reference): many transforms of uneven sizes ----
  * One task per transform, in place; twiddle is the root table of the task's size (use the
- * inverse root's table and scale_d = n^-1 for an inverse NTT, shift_d for a coset).  A plan
- * uploads the task tables once; running it launches one persistent kernel per pass (every
- * task's pencils share the launch) and one batched permutation, with no allocation or host
- * copy, so it can be captured into a CUDA graph and replayed. */
+ * inverse root's table and scale_d = n^-1 for an inverse NTT, shift_d for a coset); shoup_d
+ * optionally the zkp_ntt_shoup_table of that table (or NULL).  A plan uploads the task tables
+ * once; running it launches one persistent kernel per pass for the small tasks (every small
+ * task's pencils share the launch) and one batched permutation, and runs each task of at least
+ * 2^solo_log points (zkp_ntt_batch_set_solo_log) through its own tuned register-pass plan, as
+ * zkp_ntt_ex_shoup does.  No allocation or host copy happens at run time, so a run can be
+ * captured into a CUDA graph and replayed. */
 typedef struct ZkpNttTask {
     PolyPtr x;
     const unsigned int *twiddle;
     unsigned int log_len;
     const unsigned int *shift_d;
     const unsigned int *scale_d;
+    const unsigned int *shoup_d;
 } ZkpNttTask;
 
 typedef struct ZkpNttBatchPlan ZkpNttBatchPlan;
 
 cudaError_t zkp_ntt_batch_plan_create(const ZkpNttTask *tasks, unsigned int ntasks, ZkpNttBatchPlan **plan);
+/* Plans made after the call run tasks of at least 2^log_len points on their own (0: every
+ * task shares the persistent launches); the default is 16. */
+cudaError_t zkp_ntt_batch_set_solo_log(unsigned int log_len);
 cudaError_t zkp_ntt_batch_run(const ZkpNttBatchPlan *plan, cudaStream_t stream);
 void zkp_ntt_batch_plan_destroy(ZkpNttBatchPlan *plan);
 

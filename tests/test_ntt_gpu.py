@@ -188,6 +188,27 @@ def test_ntt_batch_uneven_sizes(zk, orc):
         assert np.array_equal(x.numpy_u64(), y.numpy_u64())
 
 
+@pytest.mark.parametrize("solo_log", [0, 1, 12, 16])
+def test_ntt_batch_solo_threshold(zk, orc, solo_log):
+    """Every split between shared persistent launches and tasks run on their own plans gives the
+    oracle's transforms (0: all shared; 1: all on their own)."""
+    lib = zk.native.load("libntt.so")
+    logs = [2, 9, 12, 14, 16, 19]
+    kinds = ["coset", "intt", "ntt", "coset", "intt", "ntt"]
+    data = [orc.gen_fr(700 + i, 1 << L) for i, L in enumerate(logs)]
+    xs = [to_dev(zk, a) for a in data]
+    try:
+        assert lib.zkp_ntt_batch_set_solo_log(solo_log) == 0
+        zk.ntt.NttBatch(list(zip(xs, kinds))).run()
+    finally:
+        assert lib.zkp_ntt_batch_set_solo_log(16) == 0
+    g = orc.to_mont(orc.int_to_limbs(7))
+    for a, x, L, kind in zip(data, xs, logs, kinds):
+        expect = {"ntt": lambda: orc.ntt(a, L), "intt": lambda: orc.intt(a, L),
+                  "coset": lambda: orc.coset_ntt(a, L, L, g)}[kind]()
+        assert np.array_equal(x.numpy_u64(), expect), (solo_log, L, kind)
+
+
 @pytest.mark.parametrize("log_n", [9, 13, 17, 20])
 def test_digit_caps_give_the_same_transform(zk, orc, log_n):
     """Every plan the tuner can pick (digit cap 4..12: more passes of smaller pencils) computes

@@ -742,7 +742,21 @@ extern "C" cudaError_t zkp_ntt_shoup_table(const unsigned int *twiddle_d, unsign
 }
 
 // ------------------------------------------------------------------ batched form
+// Tasks of at least 2^solo_log points run their own tuned plan (register passes, Shoup
+// twiddles when given) instead of the shared persistent pencil launches, which use the
+// shared-memory pass for every pass.
+namespace zk {
+namespace ntt {
+std::atomic<u32> g_batch_solo_log{16};
+}  // namespace ntt
+}  // namespace zk
+
 struct ZkpNttBatchPlan {
+    struct Solo {
+        View v;
+        u32 L;
+        const u32 *tw, *shift, *scale, *shoup;
+    };
     struct Phase {
         ntt::PassArgs *args;
         u64 *first;
@@ -758,6 +772,7 @@ struct ZkpNttBatchPlan {
     u64 *br_first = nullptr;
     u32 br_count = 0;
     u64 br_total = 0;
+    std::vector<Solo> solo;
     void *mem = nullptr;
 };
 
@@ -772,13 +787,19 @@ extern "C" cudaError_t zkp_ntt_batch_plan_create(const ZkpNttTask *tasks, unsign
     std::vector<View> br_views;
     std::vector<u32> br_logs;
     std::vector<u64> br_first{0};
+    const u32 solo_log = ntt::g_batch_solo_log.load(std::memory_order_relaxed);
     for (u32 t = 0; t < ntasks; t++) {
         const ZkpNttTask &task = tasks[t];
         const u32 L = task.log_len;
         View v;
-        if (L == 0 || L > 28 || task.x.len != (1ull << L) || task.twiddle == nullptr || !make_view(task.x, &v)) {
+        if (L == 0 || L > 28 || task.x.len != (1ull << L) || task.twiddle == nullptr || !make_view(task.x, &v) ||
+            (reinterpret_cast<uintptr_t>(task.shoup_d) & 15) != 0) {
             delete plan;
             return cudaErrorInvalidValue;
+        }
+        if (solo_log != 0 && L >= solo_log) {
+            plan->solo.push_back({v, L, task.twiddle, task.shift_d, task.scale_d, task.shoup_d});
+            continue;
         }
         const ntt::Plan p = ntt::make_plan(L, task.shift_d != nullptr, /*ignore_cap=*/true);
         for (u32 ph = 0; ph < p.np; ph++) {
@@ -827,6 +848,11 @@ extern "C" cudaError_t zkp_ntt_batch_plan_create(const ZkpNttTask *tasks, unsign
     int max_smem = 0;
     cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, plan->device);
     err = ensure_smem_attr(ntt::ntt_batch_pass_kernel, (int)ntt::pass_smem(ntt::MAX_D), ntt::g_batch_attr_done);
+    // the solo tasks' kernels get their shared-memory limits now, outside any stream capture
+    if (err == cudaSuccess && !plan->solo.empty())
+        err = ensure_smem_attr(ntt::ntt_pass_kernel, (int)ntt::pass_smem(ntt::MAX_D), ntt::g_attr_done);
+    if (err == cudaSuccess && !plan->solo.empty())
+        err = ensure_smem_attr(ntt::bitrev_tiled_kernel, (int)ntt::BR_SMEM, ntt::g_br_attr_done);
     for (size_t ph = 0; ph < args.size() && err == cudaSuccess; ph++) {
         ZkpNttBatchPlan::Phase P{};
         P.args = reinterpret_cast<ntt::PassArgs *>(base + off);
@@ -888,6 +914,14 @@ extern "C" cudaError_t zkp_ntt_batch_run(const ZkpNttBatchPlan *plan, cudaStream
                                                           plan->br_count);
         ZK_TRY(cudaGetLastError());
     }
+    for (const auto &t : plan->solo)
+        ZK_TRY(ntt::run(t.v, nullptr, 0, t.L, t.tw, nullptr, t.shift, t.scale, stream, t.shoup));
+    return cudaSuccess;
+}
+
+extern "C" cudaError_t zkp_ntt_batch_set_solo_log(unsigned int log_len) {
+    ZK_CHECK_ARG(log_len <= 29);
+    ntt::g_batch_solo_log.store(log_len);
     return cudaSuccess;
 }
 

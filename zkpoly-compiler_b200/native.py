@@ -54,6 +54,7 @@ SIGNATURES = {
         "zkp_ntt_set_max_digit": (cudaError_t, [ctypes.c_uint, ctypes.c_uint]),
         "zkp_ntt_batch_plan_create": (cudaError_t, [c_void_p, ctypes.c_uint, ctypes.POINTER(c_void_p)]),
         "zkp_ntt_batch_run": (cudaError_t, [c_void_p, c_void_p]),
+        "zkp_ntt_batch_set_solo_log": (cudaError_t, [ctypes.c_uint]),
         "zkp_ntt_batch_plan_destroy": (None, [c_void_p]),
         "zkp_ntt_profile_enable": (None, [ctypes.c_int]),
         "zkp_ntt_profile_read": (ctypes.c_int, [ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_char_p),
@@ -129,7 +130,7 @@ SIGNATURES = {
 class ZkpNttTask(ctypes.Structure):
     """include/ntt.h ZkpNttTask"""
     _fields_ = [("x", PolyPtr), ("twiddle", ctypes.c_void_p), ("log_len", ctypes.c_uint),
-                ("shift_d", ctypes.c_void_p), ("scale_d", ctypes.c_void_p)]
+                ("shift_d", ctypes.c_void_p), ("scale_d", ctypes.c_void_p), ("shoup_d", ctypes.c_void_p)]
 
 
 class ZkpMsmTask(ctypes.Structure):

@@ -215,8 +215,9 @@ class NttBatch:
             tw = twiddle_table(log_n, inverse)
             sh = scalar_const(shift) if kind == "coset" else None
             sc = n_inv(log_n) if inverse else None
-            self._keep += [x, tw, sh, sc]
-            arr[i] = ZkpNttTask(x.poly_ptr(), tw.values.data_ptr(), log_n, _ptr(sh), _ptr(sc))
+            st = shoup_table(log_n, inverse)
+            self._keep += [x, tw, sh, sc, st]
+            arr[i] = ZkpNttTask(x.poly_ptr(), tw.values.data_ptr(), log_n, _ptr(sh), _ptr(sc), st.data_ptr())
         self._plan = ctypes.c_void_p()
         self._destroy = lib.zkp_ntt_batch_plan_destroy  # kept: module globals may be gone at exit
         check(lib.zkp_ntt_batch_plan_create(ctypes.cast(arr, ctypes.c_void_p), len(tasks),
