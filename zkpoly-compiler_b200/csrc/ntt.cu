@@ -472,6 +472,79 @@ __global__ void __launch_bounds__(256) bitrev_tiled_kernel(View v, u32 L) {
 
 constexpr size_t BR_SMEM = 2 * 8 * BR_TILE * sizeof(u32);  // 64 KiB
 
+// The last register pass fused with the tiled bit reversal (L >= 2 BR_T, last digit D <= BR_T,
+// table mode).  The last pass's pencils (2^D consecutive elements, lo = 0) lie inside the rows
+// of 2^BR_T elements the tiled permutation moves, so CTA m (m <= rev m) loads the rows of tiles
+// m and rev m, runs the last pass's radix-2 stages on each row in registers (16 lanes a row,
+// two elements a lane, the register pass's lane swaps and twiddles), stores the canonical
+// results into shared memory and writes them back permuted as bitrev_tiled_kernel does.  The
+// vector is read and written once for both steps instead of twice.
+template <u32 D, bool SH>
+__global__ void __launch_bounds__(512) ntt_last_bitrev_kernel(PassArgs a) {
+    extern __shared__ u32 br_sm[];  // 2 tiles x 8 planes x BR_TILE words
+    const u32 L = a.L;
+    const u32 M = L - 2 * BR_T;
+    const u32 m = blockIdx.x;
+    const u32 mr = M ? (__brev(m) >> (32 - M)) : 0u;
+    if (mr < m) return;  // the pair is handled by CTA mr
+    const u32 ntile = mr == m ? 1 : 2;
+    constexpr u32 g = 1u << (D - 1);             // lanes per pencil
+    const u32 lane = threadIdx.x & 31;
+    const u32 u = threadIdx.x & 15;              // lane within the row
+    const u32 j = u >> (D - 1), l = u & (g - 1);  // pencil within the row, lane within the pencil
+    const bool postscale = (a.flags & F_POSTSCALE) != 0;
+    Fr scale;
+    if (postscale) scale = Fr::load_nc(a.scale);
+    for (u32 r = threadIdx.x >> 4; r < 32 * ntile; r += blockDim.x >> 4) {
+        const u32 t = r >> BR_T, ar = r & 31;    // tile, top bits of the row
+        const u64 base = ((u64)ar << (L - BR_T)) | ((u64)(t ? mr : m) << BR_T) | ((u64)j << D);
+        Fr x0 = Fr::load(a.v.at(base + l));
+        Fr x1 = Fr::load(a.v.at(base + l + g));
+#pragma unroll
+        for (int k = (int)D - 1; k >= 0; k--) {
+            if (k < (int)D - 1) lane_swap(x0, x1, lane, (u32)k);
+            const u64 e = (u64)(l & ((1u << k) - 1)) << (L - 1 - (u32)k);
+            Fr s = Fr::add(x0, x1);
+            Fr d = Fr::sub(x0, x1);
+            if (e != 0) {
+                if (SH) d = Fr::mul_shoup(d, Fr::load_nc(a.shoup + e * 16), Fr::load_nc(a.shoup + e * 16 + 8));
+                else d = Fr::mul(d, Fr::load_nc(a.tw + e * 8));
+            }
+            x0 = s;
+            x1 = d;
+        }
+        if (postscale) {
+            x0 = Fr::mul(x0, scale);
+            x1 = Fr::mul(x1, scale);
+        }
+        x0 = x0.canonical();
+        x1 = x1.canonical();
+        // local outputs 2l and 2l + 1 of pencil j are row elements b0 and b0 + 1
+        u32 *tile = br_sm + t * 8 * BR_TILE;
+        const u32 b0 = (j << D) + 2 * l;
+        const u32 p0 = ar * 32 + (b0 ^ ar), p1 = ar * 32 + ((b0 + 1) ^ ar);
+#pragma unroll
+        for (int w = 0; w < 8; w++) {
+            tile[w * BR_TILE + p0] = x0.v[w];
+            tile[w * BR_TILE + p1] = x1.v[w];
+        }
+    }
+    __syncthreads();
+    const u32 warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    for (u32 t = 0; t < ntile; t++) {
+        const u32 *src = br_sm + (ntile == 2 ? 1 - t : 0) * 8 * BR_TILE;
+        for (u32 ao = warp; ao < 32; ao += nwarp) {
+            const u32 ra = __brev(lane) >> 27, rb = __brev(ao) >> 27;
+            const u32 pos = ra * 32 + (rb ^ ra);
+            Fr x;
+#pragma unroll
+            for (int w = 0; w < 8; w++) x.v[w] = src[w * BR_TILE + pos];
+            const u64 i = ((u64)ao << (L - BR_T)) | ((u64)(t ? mr : m) << BR_T) | lane;
+            x.store(a.v.at(i));
+        }
+    }
+}
+
 __global__ void __launch_bounds__(256) distribute_powers_kernel(View v, const u32 *powers, u64 pn, u64 n) {
     const u64 stride = (u64)gridDim.x * blockDim.x;
     for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
@@ -555,6 +628,7 @@ inline Plan make_plan(u32 L, bool wide_first = false, bool ignore_cap = false) {
 std::atomic<uint64_t> g_attr_done{0};
 std::atomic<uint64_t> g_batch_attr_done{0};
 std::atomic<uint64_t> g_br_attr_done{0};
+std::atomic<uint64_t> g_lbr_attr_done[BR_T + 1][2];
 
 inline size_t pass_smem(u32 D) {
     const size_t S = 1u << D, H = S > 1 ? S / 2 : 1;
@@ -596,10 +670,51 @@ cudaError_t launch_pass(const PassArgs &a, cudaStream_t stream) {
     return cudaGetLastError();
 }
 
+// The last pass and the permutation in one kernel when the last pass is a register pass of at
+// most 2^BR_T points on at least 2^(2 BR_T) elements.
+inline bool fuse_last(const Plan &plan, u32 L, bool recompute) {
+    return plan.np > 1 && L >= 2 * BR_T && !recompute && plan.D[plan.np - 1] <= BR_T;
+}
+
+template <u32 D, bool SH>
+cudaError_t launch_last_bitrev_d(const PassArgs &a, cudaStream_t stream) {
+    ZK_TRY(ensure_smem_attr(ntt_last_bitrev_kernel<D, SH>, (int)BR_SMEM, g_lbr_attr_done[D][SH ? 1 : 0]));
+    ntt_last_bitrev_kernel<D, SH><<<1u << (a.L - 2 * BR_T), 512, BR_SMEM, stream>>>(a);
+    return cudaGetLastError();
+}
+
+template <bool SH>
+cudaError_t launch_last_bitrev(const PassArgs &a, cudaStream_t stream) {
+    switch (a.D) {
+        case 1: return launch_last_bitrev_d<1, SH>(a, stream);
+        case 2: return launch_last_bitrev_d<2, SH>(a, stream);
+        case 3: return launch_last_bitrev_d<3, SH>(a, stream);
+        case 4: return launch_last_bitrev_d<4, SH>(a, stream);
+        default: return launch_last_bitrev_d<5, SH>(a, stream);
+    }
+}
+
+// the shared-memory limits of every kernel run() may launch, set ahead of a stream capture
+inline cudaError_t prepare_run_attrs() {
+    ZK_TRY(ensure_smem_attr(ntt_pass_kernel, (int)pass_smem(MAX_D), g_attr_done));
+    ZK_TRY(ensure_smem_attr(bitrev_tiled_kernel, (int)BR_SMEM, g_br_attr_done));
+    ZK_TRY(ensure_smem_attr(ntt_last_bitrev_kernel<1, false>, (int)BR_SMEM, g_lbr_attr_done[1][0]));
+    ZK_TRY(ensure_smem_attr(ntt_last_bitrev_kernel<2, false>, (int)BR_SMEM, g_lbr_attr_done[2][0]));
+    ZK_TRY(ensure_smem_attr(ntt_last_bitrev_kernel<3, false>, (int)BR_SMEM, g_lbr_attr_done[3][0]));
+    ZK_TRY(ensure_smem_attr(ntt_last_bitrev_kernel<4, false>, (int)BR_SMEM, g_lbr_attr_done[4][0]));
+    ZK_TRY(ensure_smem_attr(ntt_last_bitrev_kernel<5, false>, (int)BR_SMEM, g_lbr_attr_done[5][0]));
+    ZK_TRY(ensure_smem_attr(ntt_last_bitrev_kernel<1, true>, (int)BR_SMEM, g_lbr_attr_done[1][1]));
+    ZK_TRY(ensure_smem_attr(ntt_last_bitrev_kernel<2, true>, (int)BR_SMEM, g_lbr_attr_done[2][1]));
+    ZK_TRY(ensure_smem_attr(ntt_last_bitrev_kernel<3, true>, (int)BR_SMEM, g_lbr_attr_done[3][1]));
+    ZK_TRY(ensure_smem_attr(ntt_last_bitrev_kernel<4, true>, (int)BR_SMEM, g_lbr_attr_done[4][1]));
+    return ensure_smem_attr(ntt_last_bitrev_kernel<5, true>, (int)BR_SMEM, g_lbr_attr_done[5][1]);
+}
+
 // Runs the full plan.  src (if non-null) is the pass-0 source for the coset LDE.
 cudaError_t run(const View &v, const View *src, u64 src_len, u32 L, const u32 *tw, const u32 *omegas,
                 const u32 *shift, const u32 *scale, cudaStream_t stream, const u32 *shoup = nullptr) {
     const Plan plan = make_plan(L, shift != nullptr || src != nullptr, omegas != nullptr);
+    const bool fused_tail = fuse_last(plan, L, omegas != nullptr);
     profiler().begin(stream);
     for (u32 p = 0; p < plan.np; p++) {
         PassArgs a{};
@@ -625,6 +740,11 @@ cudaError_t run(const View &v, const View *src, u64 src_len, u32 L, const u32 *t
         if (p == 0 && src) f |= F_SRC;
         if (omegas) f |= F_RECOMPUTE;
         a.flags = f;
+        if (fused_tail && p + 1 == plan.np) {
+            ZK_TRY(shoup ? launch_last_bitrev<true>(a, stream) : launch_last_bitrev<false>(a, stream));
+            profiler().mark("ntt_pass", stream);
+            return cudaSuccess;
+        }
         ZK_TRY(launch_pass(a, stream));
         profiler().mark("ntt_pass", stream);
     }
@@ -849,10 +969,7 @@ extern "C" cudaError_t zkp_ntt_batch_plan_create(const ZkpNttTask *tasks, unsign
     cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, plan->device);
     err = ensure_smem_attr(ntt::ntt_batch_pass_kernel, (int)ntt::pass_smem(ntt::MAX_D), ntt::g_batch_attr_done);
     // the solo tasks' kernels get their shared-memory limits now, outside any stream capture
-    if (err == cudaSuccess && !plan->solo.empty())
-        err = ensure_smem_attr(ntt::ntt_pass_kernel, (int)ntt::pass_smem(ntt::MAX_D), ntt::g_attr_done);
-    if (err == cudaSuccess && !plan->solo.empty())
-        err = ensure_smem_attr(ntt::bitrev_tiled_kernel, (int)ntt::BR_SMEM, ntt::g_br_attr_done);
+    if (err == cudaSuccess && !plan->solo.empty()) err = ntt::prepare_run_attrs();
     for (size_t ph = 0; ph < args.size() && err == cudaSuccess; ph++) {
         ZkpNttBatchPlan::Phase P{};
         P.args = reinterpret_cast<ntt::PassArgs *>(base + off);
@@ -954,6 +1071,7 @@ extern "C" unsigned int zkp_ntt_plan_digits(unsigned int log_len, unsigned int *
 
 extern "C" unsigned int zkp_ntt_num_passes(unsigned int log_len) {
     ntt::Plan p = ntt::make_plan(log_len);
+    if (ntt::fuse_last(p, log_len, false)) return p.np;  // the last pass also permutes
     return p.np + (p.np > 1 ? 1 : 0);
 }
 
