@@ -368,10 +368,31 @@ __global__ void __launch_bounds__(256) scatter_kernel(const Batch b, u32 *cursor
         const u32 kb = (u32)b.key_first[t];
         Digits d;
         load_digits(d, k.scalars + i * 8, k.c);
+        // records queue up QD at a time, so QD cursor atomics are in flight before the first of
+        // their stores waits on a returned position; the queue keeps the digits' order
+        constexpr u32 QD = 4;
+        u32 qk[QD], qv[QD], nq = 0;
+        auto flush = [&]() {
+            u32 pos[QD];
+#pragma unroll
+            for (u32 q = 0; q < QD; q++)
+                if (q < nq) pos[q] = atomicAdd(cursor + qk[q], 1u);
+#pragma unroll
+            for (u32 q = 0; q < QD; q++)
+                if (q < nq) records[pos[q]] = make_uint2(qk[q], qv[q]);
+            nq = 0;
+        };
         for_each_digit(d, k, [&](u32 table, u32 key, bool neg) {
-            const u32 pos = atomicAdd(cursor + kb + key, 1u);
-            records[pos] = make_uint2(kb + key, (u32)(table * k.stride + i) | (neg ? 0x80000000u : 0u));
+            const u32 id = kb + key, v = (u32)(table * k.stride + i) | (neg ? 0x80000000u : 0u);
+#pragma unroll
+            for (u32 q = 0; q < QD; q++)
+                if (q == nq) {
+                    qk[q] = id;
+                    qv[q] = v;
+                }
+            if (++nq == QD) flush();
         });
+        flush();
     }
 }
 
