@@ -122,6 +122,34 @@ def test_distribute_powers(zk, orc):
         assert np.array_equal(x.numpy_u64(), orc.distribute_powers(a, p)), pn
 
 
+@pytest.mark.parametrize("k", [10, 13, 16])
+def test_distribute_zeta_then_recompute_ntt(zk, orc, k):
+    """The reference's composed case (core/tests/ntt.rs:262-383): 2^k coefficients zero-extended
+    to 2^(k+2) in a view rotated by -2, multiplied periodically by [1, zeta, zeta^2]
+    (distribute_powers with three powers), then recompute_ntt at the extended size: halo2's
+    coeff_to_extended, the evaluations at zeta * w_ext^j.  halo2curves' ZETA is one of Fr's two
+    primitive cube roots; 7^((r-1)/3) is used here, the choice changes only the constant."""
+    F = zk.field
+    zeta = pow(F.GENERATOR, (F.FR_MODULUS - 1) // 3, F.FR_MODULUS)
+    assert zeta != 1 and pow(zeta, 3, F.FR_MODULUS) == 1
+    ext = k + 2
+    N = 1 << ext
+    a = orc.gen_fr(300 + k, 1 << k)
+    logical = np.zeros((N, 4), dtype=np.uint64)
+    logical[: 1 << k] = a
+    # rotate(-2): logical element i is stored at (i + 2) mod N
+    x = to_dev(zk, np.roll(logical, 2, axis=0))
+    x.rotate(-2)
+    assert np.array_equal(x.numpy_u64(), logical)
+    zm = orc.to_mont(orc.int_to_limbs(zeta))
+    powers = np.stack([orc.one(), zm, orc.mul(zm, zm)])
+    zk.ntt.distribute_powers(x, zk.ScalarArray.from_numpy(powers))
+    w = F.mont_words(F.root_of_unity(ext))
+    pq, omegas = zk.ntt.gen_pq_omegas(zk.ntt.get_pq_len(ext), N, w)
+    zk.ntt.recompute_ntt(x, zk.ScalarArray.from_numpy(pq), zk.ScalarArray.from_numpy(omegas))
+    assert np.array_equal(x.numpy_u64(), orc.coset_ntt(a, k, ext, zm))
+
+
 @pytest.mark.parametrize("log_in,log_out", [(2, 5), (10, 13), (13, 16), (16, 19)])
 def test_coset_lde(zk, orc, log_in, log_out):
     coef = orc.gen_fr(12, 1 << log_in)

@@ -163,6 +163,20 @@ def test_distribute_powers(orc):
         assert (r[i] == orc.mul(a[i], p[i % 7])).all()
 
 
+def test_zeta_periodic_powers_are_a_coset(orc):
+    """Three periodic powers [1, zeta, zeta^2] of a cube root zeta equal the coset shift by zeta
+    (zeta^(i mod 3) = zeta^i): the identity the zeta-coset extension test relies on."""
+    r = 0x30644E72E131A029B85045B68181585D2833E84879B9709143E1F593F0000001
+    zeta = orc.to_mont(I(orc, pow(7, (r - 1) // 3, r)))
+    assert not (zeta == orc.one()).all() and (orc.pow_(zeta, 3) == orc.one()).all()
+    k, ext = 4, 6
+    coef = orc.gen_fr(19, 1 << k)
+    padded = np.zeros((1 << ext, 4), dtype=np.uint64)
+    padded[: 1 << k] = coef
+    shifted = orc.distribute_powers(padded, np.stack([orc.one(), zeta, orc.mul(zeta, zeta)]))
+    assert np.array_equal(orc.ntt(shifted, ext), orc.coset_ntt(coef, k, ext, zeta))
+
+
 def test_eval_horner_and_chunked(orc):
     poly = orc.gen_fr(4, 5000)
     x = orc.gen_fr(5, 1)[0]
