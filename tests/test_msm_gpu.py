@@ -243,3 +243,26 @@ def test_msm_affine_rounds_empty_lists(zk, orc):
         assert np.array_equal(_device_msm(zk, s, p, 9), orc.best_multiexp(s, p))
     finally:
         zk.msm.set_affine_rounds(-1)
+
+
+@pytest.mark.parametrize("bits", [1, 8, 16, 32, 64, 128])
+def test_msm_narrow_scalars(zk, orc, bits):
+    """Scalars of 1..128 bits, as the reference's coefficient generator makes them
+    (core/tests/msm.rs:70-120: a 128-bit draw masked to the width, then from_u128): the high
+    windows are empty and a few buckets of the low windows take most points (1-bit scalars put
+    about half the points in one bucket), with and without pairing rounds and tables."""
+    n = 4096
+    rng = np.random.default_rng(600 + bits)
+    mask = (1 << bits) - 1
+    vals = [(int(lo) | (int(hi) << 64)) & mask for lo, hi in rng.integers(0, np.iinfo(np.uint64).max, (n, 2), dtype=np.uint64, endpoint=True)]
+    s = np.stack([orc.to_mont(orc.int_to_limbs(v)) for v in vals])
+    p = orc.gen_points(601, n)
+    expect = orc.best_multiexp(s, p)
+    for rounds in (0, 3):
+        zk.msm.set_affine_rounds(rounds)
+        try:
+            for window, n_tables in ((8, 1), (16, 1), (12, 8)):
+                assert np.array_equal(_device_msm(zk, s, p, window, n_tables), expect), (rounds, window, n_tables)
+        finally:
+            zk.msm.set_affine_rounds(-1)
+    assert np.array_equal(zk.msm.msm_host(s, p), expect)
