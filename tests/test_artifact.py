@@ -227,3 +227,28 @@ def test_gpu_constants_drive_kernels(zk, orc, tmp_path):
         assert np.array_equal(_words(res), orc.best_multiexp(scalars, pts)), n_tables
     with pytest.raises(ValueError):
         a.resident_bases(table[0])
+
+
+@pytest.mark.gpu
+def test_gpu_constants_feed_the_server(zk, tmp_path):
+    """A served prover built on point bases loaded from an artifact gives the same results as one
+    built on the same bases generated in HBM."""
+    a = zk.artifact
+    pts = zk.gen.points(2, 1 << 12)
+    a.dump_constant_table(str(tmp_path), [a.Constant("srs", a.point_base_typ(1 << 12), a.gpu_device(0), pts)])
+    loaded = a.by_name(a.load_constant_table(str(tmp_path)), "srs").value
+    assert torch.equal(loaded, pts)
+    results = []
+    for bases in (pts, loaded):
+        srv = zk.serving.Server(bases, hbm_bytes=2 << 30, max_inflight=2, ext_log=2, min_k=10, max_k=12)
+        try:
+            got = []
+            for k, seed in ((10, 1), (12, 2)):
+                r = srv.wait(srv.submit(k, seed))
+                assert r.status == 0
+                got.append(zk.serving.result_words(r))
+            results.append(got)
+        finally:
+            srv.close()
+    for x, y in zip(*results):
+        assert np.array_equal(x, y)
