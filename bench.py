@@ -29,6 +29,18 @@ sys.path.insert(0, ROOT)
 
 METRIC = "MSM points/s (2^22) & NTT elems/s (2^24); served p50/p99 vs plain per-call"
 MSM_LOG, NTT_LOG = 22, 24
+# ncu DRAM bytes (read + write) of one whole 2^22 transform (all passes) per element, from the
+# capture summarised in profiles/ntt_passes_ntt2p22.md; traffic grows with the element count
+NTT_TRAFFIC_PER_ELEM = 342.0
+
+
+def workload_config(world: int) -> dict:
+    """The workload both arms report (the GPU arm's resident-table choice is under "msm")."""
+    return {"workload": f"MSM n=2^{MSM_LOG} (BN254 G1, seeded scalars, points k_i*G) + NTT n=2^{NTT_LOG} "
+                        f"(BN254 Fr, natural order, seeded)",
+            "msm_n": 1 << MSM_LOG, "ntt_n": 1 << NTT_LOG, "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2 (NTT 512 MiB vector; MSM bases, sorted digits and pairing lists "
+                  "of hundreds of MB to GBs)"}
 
 
 def dist_env():
@@ -127,20 +139,69 @@ def cpu_reference(sample_msm_log=22, sample_ntt_log=24, reps=1):
     s, p, a = _CPU_INPUTS[key]
     t0 = time.perf_counter()
     for _ in range(reps):
-        orc.best_multiexp(s, p)
+        msm_out = orc.best_multiexp(s, p)
     msm_t = (time.perf_counter() - t0) / reps
     w = orc.root_of_unity(sample_ntt_log)
     t0 = time.perf_counter()
     for _ in range(reps):
-        orc.best_fft(a, w, sample_ntt_log)
+        ntt_out = orc.best_fft(a, w, sample_ntt_log)
     ntt_t = (time.perf_counter() - t0) / reps
     return {
         "msm_points_per_s": (1 << sample_msm_log) / msm_t,
         "ntt_elems_per_s": (1 << sample_ntt_log) / ntt_t,
         "cores": th,
+        "msm_s": msm_t, "ntt_s": ntt_t,
         "msm_sample": f"best_multiexp n=2^{sample_msm_log} (seeds 1/2), {msm_t:.2f} s",
         "ntt_sample": f"best_fft n=2^{sample_ntt_log} (seed 0), {ntt_t:.2f} s",
+        # the outputs themselves: the GPU arm checks its timed results against them
+        "logs": (sample_msm_log, sample_ntt_log), "msm_out": msm_out, "ntt_out": ntt_out, "ntt_in": a,
     }
+
+
+def ntt_chain_expected(a, fft_a, t: int, log_n: int):
+    """State of a vector after t in-place forward transforms, from one transform of it.
+
+    Applying the size-n DFT twice gives F(F(a))[j] = n * a[-j mod n], so after t transforms
+    the vector is n^m * b[(-1)^m j mod n] with m = t // 2 and b = a (t even) or F(a) (t odd).
+    This lets the benchmark check the exact bytes its timed in-place transforms left behind
+    against one best_fft of the input."""
+    import numpy as np
+    from oracle import oracle as orc
+    n = 1 << log_n
+    m = t // 2
+    b = fft_a if t % 2 else a
+    if m % 2:
+        idx = (-np.arange(n, dtype=np.int64)) % n
+        b = b[idx]
+    if m:
+        nm = orc.pow_(orc.to_mont(orc.int_to_limbs(n)), m)
+        b = orc.vec_mul(np.ascontiguousarray(b), np.ascontiguousarray(np.broadcast_to(nm, b.shape)))
+    return np.ascontiguousarray(b)
+
+
+def verify_outputs(cpu, timed, e2e):
+    """Bit-exact comparison of the timed results (and of the C-ABI e2e results) with the CPU
+    port's best_multiexp / best_fft on the same seeded inputs."""
+    import numpy as np
+    from oracle import oracle as orc
+    if cpu is None or cpu["logs"] != (MSM_LOG, NTT_LOG):
+        orc.build()
+        s, p = orc.gen_fr(1, 1 << MSM_LOG), orc.gen_points(2, 1 << MSM_LOG)
+        a = orc.gen_fr(0, 1 << NTT_LOG)
+        cpu = {"msm_out": orc.best_multiexp(s, p), "ntt_in": a,
+               "ntt_out": orc.best_fft(a, orc.root_of_unity(NTT_LOG), NTT_LOG)}
+    out = {}
+    out["msm_timed"] = bool(np.array_equal(timed["msm"], cpu["msm_out"]))
+    expect = ntt_chain_expected(cpu["ntt_in"], cpu["ntt_out"], timed["ntt_transforms"], NTT_LOG)
+    out["ntt_timed"] = bool(np.array_equal(timed["ntt"], expect))
+    if e2e is not None:
+        out["msm_e2e"] = bool(np.array_equal(e2e["msm"], cpu["msm_out"]))
+        out["ntt_e2e"] = bool(np.array_equal(e2e["ntt"], cpu["ntt_out"]))
+    out["how"] = (f"MSM result of the last timed step and of the e2e msm() call == best_multiexp (seeds 1/2, "
+                  f"n=2^{MSM_LOG}); NTT vector after the {timed['ntt_transforms']} in-place transforms of "
+                  f"warm-up + timed region == n^m * best_fft(a)[(-1)^m j] (m = t // 2; F(F(a))[j] = n a[-j]); "
+                  f"e2e ssip_ntt output == best_fft(a) (seed 0, n=2^{NTT_LOG})")
+    return all(v for k, v in out.items() if k != "how"), out
 
 
 def run_reference_arm(args):
@@ -158,12 +219,11 @@ def run_reference_arm(args):
         "impl": "reference", "metric": METRIC, "value": v, "unit": "points/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32 (BN254 Montgomery limbs)", "data": "synthetic (seeded)",
-        "config": {"workload": f"MSM n=2^{MSM_LOG} + NTT n=2^{NTT_LOG} (BN254), CPU sample "
-                               f"MSM 2^{args.ref_msm_log} / NTT 2^{args.ref_ntt_log}",
-                   "cpu": cpu_model()},
+        "config": workload_config(world),
+        "ms_per_step": statistics.median([s["msm_s"] + s["ntt_s"] for s in steps]) * 1e3,
         "ntt": {"metric": f"NTT elems/s (2^{NTT_LOG})", "value": ntt_v, "unit": "elems/s"},
         "cpu_baseline": {"value": v, "unit": "points/s", "cores": steps[-1]["cores"], "kind": "port",
-                         "sample": steps[-1]["msm_sample"] + "; " + steps[-1]["ntt_sample"]},
+                         "sample": steps[-1]["msm_sample"] + "; " + steps[-1]["ntt_sample"], "cpu": cpu_model()},
         "e2e": {"value": v, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -240,6 +300,14 @@ def run_gpu(args):
     ntt_ms = ev[0].elapsed_time(ev[1]) / args.steps
     msm_ms = ev[1].elapsed_time(ev[2]) / args.steps
     step_ms = ntt_ms + msm_ms
+    # the timed region's own results, kept for the bit-exact check against the CPU port: the
+    # MSM result of the last timed step, and the vector the warm-up + timed in-place
+    # transforms left behind
+    timed_out = None
+    if rank == 0 and not args.no_verify:
+        timed_out = {"msm": res.cpu().numpy().view(np.uint64).copy(),
+                     "ntt": x.values.cpu().numpy().view(np.uint64).reshape(n_ntt, 4).copy(),
+                     "ntt_transforms": args.warmup + args.steps}
     # the same transform through ssip_ntt (every rank runs it, outside the timed region)
     for _ in range(2):
         ssip_step()
@@ -324,17 +392,22 @@ def run_gpu(args):
 
     # ---- e2e through the reference C ABI from pinned host memory
     e2e_msm_s = e2e_ntt_s = float("nan")
+    e2e_out = None
     if not args.no_e2e:
-        e2e_msm_s, e2e_ntt_s = run_e2e(zk, native, lib_msm, scalars, points, ntt_in, tw, stream, dev, local, args,
-                                       n_msm, n_ntt)
+        e2e_msm_s, e2e_ntt_s, e2e_out = run_e2e(zk, native, lib_msm, scalars, points, ntt_in, tw, stream, dev,
+                                                local, args, n_msm, n_ntt)
 
     # ---- CPU baseline (rank 0 at N=1)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_reference(args.ref_msm_log, args.ref_ntt_log)
+    # ---- the timed and e2e results against the CPU port, bit for bit (rank 0)
+    verified = None
+    if timed_out is not None:
+        verified = verify_outputs(cpu, timed_out, e2e_out if rank == 0 else None)
     emit(args, zk, rank, world, n_msm, n_ntt, ntt_ms, msm_ms, step_ms, pass_ms, bitrev_ms, stage_ms, imad_per_s,
          e2e_msm_s, e2e_ntt_s, cpu, clocks, bases, batched, served, fused, mont_per_s, poly, pipelined,
-         ssip_ms, shoup_per_s)
+         ssip_ms, shoup_per_s, verified)
 
 
 def measure_fused(zk, gen, dev, stream, hbm_peak, mont_peak, shoup_peak, log_n=NTT_LOG, ext=3, reps=10):
@@ -619,12 +692,14 @@ def run_e2e(zk, native, lib_msm, scalars, points, ntt_in, tw, stream, dev, local
             e2e_ntt()
         stream.synchronize()
         t2 = time.perf_counter()
-    return (t1 - t0) / args.steps, (t2 - t1) / args.steps
+    # the last e2e call's results, as the caller received them in host memory
+    outs = {"msm": result.view(np.uint64).copy(), "ntt": h_out.numpy().view(np.uint64).reshape(n_ntt, 4).copy()}
+    return (t1 - t0) / args.steps, (t2 - t1) / args.steps, outs
 
 
 def emit(args, zk, rank, world, n_msm, n_ntt, ntt_ms, msm_ms, step_ms, pass_ms, bitrev_ms, stage_ms, imad_per_s,
          e2e_msm_s, e2e_ntt_s, cpu, clocks, bases, batched=None, served=None, fused=None, mont_per_s=None,
-         poly=None, pipelined=None, ssip_ms=None, shoup_per_s=None):
+         poly=None, pipelined=None, ssip_ms=None, shoup_per_s=None, verified=None):
     import torch
     if rank != 0:
         if world > 1:
@@ -636,6 +711,8 @@ def emit(args, zk, rank, world, n_msm, n_ntt, ntt_ms, msm_ms, step_ms, pass_ms, 
     # the profiling runs record every pass of each transform
     pass_total = sum(pass_ms) / max(1, len(pass_ms) // max(1, len(zk.ntt.plan_digits(NTT_LOG))))
     ntt_bytes_per_pass = 64 * n_ntt  # one read + one write of every element per pass
+    ntt_alg_bytes = 64 * n_ntt       # algorithmic bytes of the whole transform
+    ntt_alg_gbs = ntt_alg_bytes / (ntt_ms / 1e3) / 1e9
     # bucket accumulation = the affine pairing rounds (pair_*) + the XYZZ walk (accumulate)
     acc_ms = sum(v for k, v in stage_ms.items() if k.startswith("pair_") or k == "accumulate")
     c_msm = bases.window
@@ -669,15 +746,13 @@ def emit(args, zk, rank, world, n_msm, n_ntt, ntt_ms, msm_ms, step_ms, pass_ms, 
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32 (BN254 Montgomery limbs, exact)",
         "data": "synthetic (seeded counter-based generator; points k_i*G)",
-        "config": {"workload": f"MSM n=2^{MSM_LOG} (BN254 G1, resident bases, window {bases.window}, "
-                               f"{bases.n_tables} precomputed tables) + "
-                               f"NTT n=2^{NTT_LOG} (BN254 Fr, natural order)",
-                   "msm_n": n_msm, "ntt_n": n_ntt, "window": bases.window, "msm_tables": bases.n_tables,
-                   "parallelism": f"replicas x{world}",
-                   "l2": f"inputs larger than L2 (NTT 512 MiB; MSM {bases.n_tables} tables of 256 MiB, 504 MB of "
-                         f"sorted digits, pairing lists of 2 GB and less)"},
+        "config": workload_config(world),
         "msm": {"metric": f"MSM points/s (2^{MSM_LOG})", "value": world * n_msm / (msm_ms / 1e3),
-                "ms": msm_ms, "stages_ms": stage_ms},
+                "ms": msm_ms, "stages_ms": stage_ms, "window": bases.window, "tables": bases.n_tables,
+                "pairing_rounds": rounds,
+                "path": f"resident bases with {bases.n_tables} precomputed tables of 2^{MSM_LOG} points, window "
+                        f"{bases.window}, {rounds} affine pairing rounds; tables built once outside the timed "
+                        f"region"},
         "ntt": {"metric": f"NTT elems/s (2^{NTT_LOG})", "value": world * n_ntt / (ntt_ms / 1e3), "unit": "elems/s",
                 "ms": ntt_ms, "pass_ms": pass_avg, "bitrev_ms": statistics.median(bitrev_ms) if bitrev_ms else None,
                 "hbm_frac_whole_ntt": (64 * n_ntt / (ntt_ms / 1e3) / 1e9) / hbm_peak,
@@ -685,14 +760,23 @@ def emit(args, zk, rank, world, n_msm, n_ntt, ntt_ms, msm_ms, step_ms, pass_ms, 
                         "table of 64 B per root, both built once outside the timed region)",
                 "ssip_ms": ssip_ms, "ssip_value": world * n_ntt / (ssip_ms / 1e3) if ssip_ms else None,
                 "ssip_path": "ssip_ntt (reference ABI): the same passes with Montgomery twiddle products"},
-        "roofline": {"kernel": f"ntt_warp_pass_kernel (register passes of 2^d-point pencils, d = {digits}, "
-                               f"of the 2^{NTT_LOG} NTT; Shoup twiddle products)", "bound": "hbm",
-                     "achieved": ntt_bytes_per_pass / (pass_avg / 1e3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
-                     "frac": ntt_bytes_per_pass / (pass_avg / 1e3) / 1e9 / hbm_peak, "peak_source": peak_kind,
-                     # ncu DRAM bytes per pass launch: 68.4 B per element at 2^22 (three Shoup
-                     # register passes and the fused last pass, 1148 MB), scaled by the element count
-                     "traffic": 68.4 * n_ntt,
-                     "note": "IMAD-bound kernel: HBM fraction reported as asked; see int_roofline"},
+        # the NTT's roofline by north_star's accounting: 64 B per element (one read + one write
+        # of the vector) for the whole transform, over the transform's CUDA-event time
+        "roofline": {"kernel": f"NTT 2^{NTT_LOG} forward transform: {len(digits)} register passes "
+                               f"(ntt_warp_pass_kernel, the last fused with the bit reversal in "
+                               f"ntt_last_bitrev_kernel), digits {digits}, Shoup twiddle products",
+                     "bound": "imad", "achieved": ntt_alg_gbs, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": ntt_alg_gbs / hbm_peak, "peak_source": peak_kind,
+                     "bytes_per_launch": ntt_alg_bytes, "launch": "one whole transform (all passes)",
+                     # ncu DRAM bytes of all passes of one transform, per element, scaled to 2^24
+                     "traffic": NTT_TRAFFIC_PER_ELEM * n_ntt,
+                     "frac_per_pass": ntt_bytes_per_pass / (pass_avg / 1e3) / 1e9 / hbm_peak,
+                     "frac_per_pass_note": "64 B per element for ONE pass over the median pass time: every pass "
+                                           "reads and writes the vector, so this credits each pass with the "
+                                           "transform's algorithmic bytes",
+                     "note": "bound by the integer multiply pipe, not HBM: the twiddle products at the measured "
+                             "Shoup-product peak take longer than the vector's HBM traffic; the binding fraction "
+                             "is int_roofline.ntt_passes.frac"},
         "int_roofline": {
             # denominator: Montgomery products per second of the library's own product routine
             # (zkp_mont_probe, measured in this run); the raw IMAD rate is listed beside it
@@ -732,6 +816,8 @@ def emit(args, zk, rank, world, n_msm, n_ntt, ntt_ms, msm_ms, step_ms, pass_ms, 
         line["batched"] = batched
     if served:
         line["served"] = served
+    if verified is not None:
+        line["verified"], line["verification"] = verified
     if cpu:
         line["cpu_baseline"] = {"value": cpu["msm_points_per_s"], "unit": "points/s", "cores": cpu["cores"],
                                 "kind": "port", "sample": cpu["msm_sample"] + "; " + cpu["ntt_sample"],
@@ -759,6 +845,8 @@ def main():
     ap.add_argument("--ref-ntt-log", type=int, default=24)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer C-ABI leg (profiling runs)")
+    ap.add_argument("--no-verify", action="store_true",
+                    help="skip the bit-exact check of the timed results against the CPU port (profiling runs)")
     ap.add_argument("--ntt-log", type=int, default=24)
     ap.add_argument("--msm-log", type=int, default=22)
     args = ap.parse_args()

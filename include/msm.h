@@ -101,8 +101,12 @@ cudaError_t zkp_msm_precompute_device(unsigned int *tables_d, unsigned long long
  * with the default window (2^16 points need 68.8 MiB); larger problems return
  * cudaErrorInvalidValue without touching the device.  The call allocates nothing.  Nothing in
  * the array has to start at zero: each call clears the counters, bucket sums and flags it uses,
- * on its stream, before its kernels read them.  Its first call on a device looks up that
- * device's copy of the array, so make that first call before any stream capture.  Every call
+ * on its stream, before its kernels read them.  The array has one copy per CUDA context: the
+ * first call in each context (the runtime's primary context of a device, or a context the host
+ * made current through the driver API) looks up that context's copy and caches it under the
+ * context's id, so a new context after cudaDeviceReset gets its own lookup.  Make that first
+ * call before any stream capture: a call that would need the lookup while its stream is being
+ * captured returns cudaErrorStreamCaptureUnsupported and does nothing.  Every call in a context
  * shares the one array, which keeps the last call's contents: calls that overlap on the GPU
  * (other streams, other host threads) race, so serialise them on one stream. */
 cudaError_t zkp_msm_device_noalloc(const unsigned int *points_d, unsigned int n_tables,

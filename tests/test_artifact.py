@@ -198,6 +198,12 @@ def test_loader_errors(zk, orc, tmp_path):
     with pytest.raises(ValueError, match="needs"):
         a.dump_constant_table(str(tmp_path / "len"), [a.Constant("r", a.scalar_array_typ(9), "CPU",
                                                                  orc.gen_fr(1, 8))])
+    # a scalar is written only from host memory (the reference panics "scalar must be on CPU"),
+    # checked before any file is written
+    for dev in (a.gpu_device(0), "Disk"):
+        with pytest.raises(ValueError, match="scalar must be on CPU"):
+            a.dump_constant_table(str(tmp_path / "sc"), [a.Constant("s", "Scalar", dev, orc.gen_fr(1, 1)[0])])
+        assert not (tmp_path / "sc").exists()
 
 
 @pytest.mark.gpu

@@ -158,8 +158,6 @@ def test_reference_msm_one_table_matches(zk, log_n):
 def test_reference_msm_precomputed_matches(zk, log_n):
     """The reference cost model's configuration for 2^22 points (window 17, 8 target windows:
     two point tables built by the reference's msm_precompute, 16 parts, two stages)."""
-    if log_n == 22 and not TIMING:
-        pytest.skip("2^22 runs with ZKP_REF_TIMING=1")
     ref = _ref_msm("libref_msm_17_8.so")
     n = 1 << log_n
     pts_dev = zk.gen.points(2, n)

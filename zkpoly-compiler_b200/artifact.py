@@ -215,6 +215,11 @@ def load_constant_table(directory: str, table: list[Constant] | None = None,
 def dump_constant_table(directory: str, table: list[Constant]) -> dict:
     """Write ``table`` as constants-manifest.json + constants.bin (``Header::build`` and
     ``dump_entries_data``, serialization.rs:175-220) and return the header."""
+    for c in table:
+        # the reference writes a scalar only from host memory (dump_binary panics with "scalar
+        # must be on CPU", serialization.rs:47-50), so no artifact it reads back holds another
+        if typ_kind(c.typ) == "Scalar" and c.device != "CPU":
+            raise ValueError(f"constant {c.name!r}: scalar must be on CPU, not {c.device!r}")
     os.makedirs(directory, exist_ok=True)
     entries, offset = [], 0
     for c in table:

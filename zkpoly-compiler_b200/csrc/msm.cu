@@ -1613,22 +1613,71 @@ static constexpr unsigned long long kNoAllocScratchBytes = 64ull << 20;  // 64 M
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
 // Host code must not use `g_noalloc_scratch` as a device address (on the host it names a
-// stand-in), so each device's real address is looked up once, with that device current.
-static std::mutex g_noalloc_mu;
-static void *g_noalloc_ptr[64] = {nullptr};
+// stand-in).  The array's real address belongs to a CUDA context, not to a device: a host that
+// makes its own driver-API context current, or a cudaDeviceReset, brings a new context with its
+// own copy of the array.  So the address is looked up with the calling context current and
+// cached under that context's unique id (cuCtxGetId ids are never reused within a process).
+using CtxGetCurrentFn = int (*)(void **ctx);
+using CtxGetIdFn = int (*)(void *ctx, unsigned long long *id);
 
-static cudaError_t noalloc_scratch(void **out) {
-    int dev = 0;
-    ZK_TRY(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> g(g_noalloc_mu);
-    if (!g_noalloc_ptr[dev]) {
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return e;
-        g_noalloc_ptr[dev] = p;
+struct NoAllocEntry {
+    unsigned long long ctx_id;
+    void *ptr;
+};
+static std::mutex g_noalloc_mu;
+static NoAllocEntry g_noalloc_cache[64];
+static unsigned g_noalloc_used = 0, g_noalloc_next = 0;
+
+static cudaError_t current_context_id(unsigned long long *id) {
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        cudaDriverEntryPointQueryResult q;
+        void *f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<CtxGetIdFn>(f);
+    });
+    if (!get_current || !get_id) return cudaErrorNotSupported;
+    void *ctx = nullptr;
+    if (get_current(&ctx) != 0) return cudaErrorDeviceUninitialized;
+    if (!ctx) {
+        // no context current yet on this thread: the runtime's own rule applies, the current
+        // device's primary context (cudaSetDevice initialises it and makes it current)
+        int dev = 0;
+        ZK_TRY(cudaGetDevice(&dev));
+        ZK_TRY(cudaSetDevice(dev));
+        if (get_current(&ctx) != 0 || !ctx) return cudaErrorDeviceUninitialized;
     }
-    *out = g_noalloc_ptr[dev];
+    if (get_id(ctx, id) != 0) return cudaErrorDeviceUninitialized;
+    return cudaSuccess;
+}
+
+static cudaError_t noalloc_scratch(cudaStream_t stream, void **out) {
+    unsigned long long id = 0;
+    ZK_TRY(current_context_id(&id));
+    std::lock_guard<std::mutex> g(g_noalloc_mu);
+    for (unsigned i = 0; i < g_noalloc_used; i++)
+        if (g_noalloc_cache[i].ctx_id == id) {
+            *out = g_noalloc_cache[i].ptr;
+            return cudaSuccess;
+        }
+    // first call in this context: the lookup is not a stream operation, so it is not made
+    // while the stream is being captured into a graph
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    ZK_TRY(cudaStreamIsCapturing(stream, &cap));
+    if (cap != cudaStreamCaptureStatusNone) return cudaErrorStreamCaptureUnsupported;
+    void *p = nullptr;
+    ZK_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    // a full cache (64 live contexts) replaces its entries in turn
+    unsigned slot = g_noalloc_used < 64 ? g_noalloc_used++ : (g_noalloc_next++ % 64);
+    g_noalloc_cache[slot] = {id, p};
+    *out = p;
     return cudaSuccess;
 }
 
@@ -1651,6 +1700,6 @@ extern "C" cudaError_t zkp_msm_device_noalloc(const unsigned int *points_d, unsi
     // larger problems do not fit the fixed scratch: refuse instead of overrunning it
     if (l.total > kNoAllocScratchBytes) return cudaErrorInvalidValue;
     void *scratch = nullptr;
-    ZK_TRY(noalloc_scratch(&scratch));
+    ZK_TRY(noalloc_scratch(stream, &scratch));
     return msm::run_batch(b, l, reinterpret_cast<char *>(scratch), stream);
 }
