@@ -92,6 +92,96 @@ void zkp_serve_stats(const ZkpServer *s, ZkpServeStats *out);
 double zkp_serve_now(const ZkpServer *s);
 void zkp_serve_destroy(ZkpServer *s);
 
+/* ---- compiled programs (the served form of a compiled artifact's instruction chunk)
+ * The reference's runtime interprets a program's instruction chunk (runtime/src/runtime.rs:
+ * 210-520 over InstructionNode, runtime/src/instructions.rs:51-178).  Here the host side
+ * (program.py) resolves a chunk's variables once - allocations to offsets inside a request's
+ * device block (HBM arena) or host block (pinned, per slot), rotations / slices / loaded
+ * constants / inputs to views - and lowers every data-moving or computing instruction to one
+ * ZkpProgOp below.  The served loop then admits requests of that program by its planned
+ * device footprint and runs its ops in order on the request's stream, so requests of
+ * different programs and sizes overlap on the GPU like the built-in prover program. */
+
+#define ZKP_PROG_MAX_VIEWS 16
+
+enum ZkpProgSpace {
+    ZKP_SPACE_NONE = 0,
+    ZKP_SPACE_DEVICE = 1,   /* byte offset inside the request's device block */
+    ZKP_SPACE_HOST = 2,     /* byte offset inside the request's pinned host block */
+    ZKP_SPACE_ABS = 3,      /* absolute device address (a resident constant) */
+    ZKP_SPACE_INPUT = 4     /* byte offset inside the request's input buffer `index` (host) */
+};
+
+/* a polynomial / scalar / buffer operand: element i is at
+ * base + ((i + offset + whole_len - rotate) mod whole_len) * elem_bytes (PolyPtr rules) */
+typedef struct ZkpProgView {
+    unsigned int space;
+    unsigned int index;
+    unsigned long long addr;
+    unsigned long long len, rotate, offset, whole_len;
+} ZkpProgView;
+
+enum ZkpProgOpKind {
+    ZKP_OP_COPY = 1,            /* v0 <- v1 element by element; imm0 = element bytes (32, 64) */
+    ZKP_OP_ZERO = 2,            /* v0 <- 0; imm0 = element bytes */
+    ZKP_OP_NTT = 3,             /* NttPrcompute: v0 poly, v1 root table (ABS); imm0 = Shoup table (ABS) or 0 */
+    ZKP_OP_NTT_RECOMPUTE = 4,   /* NttRecompute: v0 poly, v1 pq, v2 omegas; imm0 = pq_deg */
+    ZKP_OP_DISTRIBUTE = 5,      /* DistributePowers: v0 poly, v1 powers */
+    ZKP_OP_FUSED = 6,           /* FusedArith: imm0 = kernel function, imm1 = num_vars, imm2 = num_mut_vars,
+                                   imm3 = len; v[0..nv) vars, v[nv..nv+nm) mut vars; v14 = device argument
+                                   buffer, v15 = host staging (both sized for the PolyPtr arrays) */
+    ZKP_OP_MSM = 7,             /* Msm: imm0 = tables (ABS), imm1 = n_tables | window << 16, imm2 = rows,
+                                   imm3 = tasks m <= 7; v[0..m) scalars, v[m..2m) results (64 B each),
+                                   v15 = device workspace */
+    ZKP_OP_EVAL = 8,            /* EvaluatePoly: v0 temp, v1 res, v2 poly, v3 x */
+    ZKP_OP_INVERT = 9,          /* BatchedInvert: v0 temp, v1 poly */
+    ZKP_OP_KATE = 10,           /* KateDivision: v0 temp, v1 q, v2 p, v3 b */
+    ZKP_OP_SCAN = 11,           /* the scan of ScanMul (its two copies are COPY ops): v0 temp, v1 target */
+    ZKP_OP_ADD = 12,            /* PolyAdd: v0 r, v1 a, v2 b */
+    ZKP_OP_SUB = 13,            /* PolySub: v0 r, v1 a, v2 b */
+    ZKP_OP_ZERO_POLY = 14,      /* NewZero: v0 */
+    ZKP_OP_ONE_LAGRANGE = 15,   /* NewOneLagrange: v0 */
+    ZKP_OP_ONE_COEF = 16,       /* NewOneCoef: v0 */
+    ZKP_OP_SCALAR_INV = 17,     /* ScalarInvert: v0 */
+    ZKP_OP_SCALAR_POW = 18      /* ScalarPow: v0; imm0 = exponent */
+};
+
+typedef struct ZkpProgOp {
+    unsigned int kind;
+    unsigned int n_views;
+    unsigned long long imm[4];
+    ZkpProgView v[ZKP_PROG_MAX_VIEWS];
+} ZkpProgOp;
+
+/* one returned value: `bytes` bytes at `host_offset` of the host block, copied into the
+ * caller's result buffer at `result_offset` when the request completes */
+typedef struct ZkpProgOut {
+    unsigned long long host_offset, bytes, result_offset;
+} ZkpProgOut;
+
+typedef struct ZkpProgram ZkpProgram;
+
+/* Registers a lowered program with the server (the ops are copied; the absolute addresses
+ * they name must stay valid while the program exists).  device_bytes is the planned HBM
+ * footprint of one request, host_bytes its pinned host block, input_bytes[i] the size of the
+ * host buffer input i must hold.  Fails with cudaErrorInvalidValue on a malformed op
+ * (unknown kind, too many views, a view outside its block or input, an output outside the
+ * host block). */
+cudaError_t zkp_serve_program_create(ZkpServer *s, const ZkpProgOp *ops, unsigned int n_ops,
+                                     unsigned long long device_bytes, unsigned long long host_bytes,
+                                     const ZkpProgOut *outs, unsigned int n_outs,
+                                     const unsigned long long *input_bytes, unsigned int n_inputs,
+                                     ZkpProgram **out);
+/* Non-blocking, like zkp_serve_submit: inputs[0..n_inputs) are host buffers (of at least the
+ * registered sizes) the program's LoadInput instructions read, `results` receives the outputs
+ * (results_bytes >= the outputs' extent, else cudaErrorInvalidValue is the request's error and
+ * status -1); both must stay valid until the request completes (zkp_serve_wait).  The
+ * request's ZkpProverResult carries status, times and footprint; msm / evals are unused. */
+long long zkp_serve_submit_program(ZkpServer *s, const ZkpProgram *prog, const void *const *inputs,
+                                   unsigned int n_inputs, void *results, unsigned long long results_bytes);
+/* Destroys a program; no request of it may be pending or running. */
+void zkp_serve_program_destroy(ZkpServer *s, ZkpProgram *prog);
+
 #ifdef __cplusplus
 }
 #endif

@@ -5,5 +5,5 @@ these modules are the host-side mirror of the reference's Rust operator wrappers
 provides device memory and streams only.
 """
 from . import field, native, scalar  # noqa: F401
-from . import artifact, batched, fused, gen, msm, ntt, pipeline, poly, serving, tuner  # noqa: F401
+from . import artifact, batched, fused, gen, msm, ntt, pipeline, poly, program, serving, tuner  # noqa: F401
 from .scalar import ScalarArray  # noqa: F401

@@ -120,11 +120,23 @@ struct Request {
     size_t off = SIZE_MAX, bytes = 0;
     int slot = -1;
     bool done = false;
+    // a request of a compiled program (null for the built-in prover program)
+    const ZkpProgram *prog = nullptr;
+    std::vector<const void *> inputs;
+    void *results = nullptr;
 };
 
 using FusedFn = cudaError_t (*)(const ConstPolyPtr *, const PolyPtr *, unsigned long long, bool, void *, cudaStream_t);
 
 }  // namespace
+
+struct ZkpProgram {
+    std::vector<ZkpProgOp> ops;
+    u64 device_bytes = 0, host_bytes = 0, result_extent = 0;
+    std::vector<ZkpProgOut> outs;
+    std::vector<u64> input_bytes;
+    std::atomic<long long> live{0};  // requests submitted and not yet completed
+};
 
 struct ZkpServer {
     ZkpServeConfig cfg{};
@@ -146,6 +158,8 @@ struct ZkpServer {
         cudaStream_t stream = nullptr;
         cudaEvent_t done = nullptr;
         u32 *host = nullptr;    // pinned: results (4*16 + 2*8 words) + PolyPtr staging
+        char *prog_host = nullptr;  // pinned host block of compiled-program requests
+        size_t prog_host_bytes = 0;
         Request *req = nullptr;
     };
     std::vector<Slot> slots;
@@ -266,7 +280,208 @@ cudaError_t launch_program(ZkpServer *s, Request *r, ZkpServer::Slot &slot) {
     return cudaSuccess;
 }
 
+// ------------------------------------------------------------------ compiled programs
+// Element size of view j of an op: buffers (temps, workspaces, argument buffers) count bytes,
+// MSM results and COPY / ZERO of points 64 bytes, everything else a 32-byte field element.
+u64 view_elem_bytes(const ZkpProgOp &op, u32 j) {
+    switch (op.kind) {
+        case ZKP_OP_COPY:
+        case ZKP_OP_ZERO:
+            return op.imm[0];
+        case ZKP_OP_FUSED:
+            return j >= 14 ? 1 : 32;
+        case ZKP_OP_MSM:
+            if (j == 15) return 1;
+            return j >= op.imm[3] ? 64 : 32;
+        case ZKP_OP_EVAL:
+        case ZKP_OP_INVERT:
+        case ZKP_OP_KATE:
+        case ZKP_OP_SCAN:
+            return j == 0 ? 1 : 32;
+        default:
+            return 32;
+    }
+}
+
+bool view_well_formed(const ZkpProgView &v) {
+    if (v.len == 0 && v.whole_len == 0) return true;
+    return v.whole_len >= v.len && v.whole_len > 0 && v.offset < v.whole_len && v.rotate < v.whole_len;
+}
+
+// the op's views that must be present (kind-specific count)
+u32 required_views(const ZkpProgOp &op) {
+    switch (op.kind) {
+        case ZKP_OP_COPY: return 2;
+        case ZKP_OP_ZERO: return 1;
+        case ZKP_OP_NTT: return 2;
+        case ZKP_OP_NTT_RECOMPUTE: return 3;
+        case ZKP_OP_DISTRIBUTE: return 2;
+        case ZKP_OP_FUSED: return (u32)(op.imm[1] + op.imm[2]);
+        case ZKP_OP_MSM: return (u32)(2 * op.imm[3]);
+        case ZKP_OP_EVAL: return 4;
+        case ZKP_OP_INVERT: return 2;
+        case ZKP_OP_KATE: return 4;
+        case ZKP_OP_SCAN: return 2;
+        case ZKP_OP_ADD:
+        case ZKP_OP_SUB: return 3;
+        case ZKP_OP_ZERO_POLY:
+        case ZKP_OP_ONE_LAGRANGE:
+        case ZKP_OP_ONE_COEF:
+        case ZKP_OP_SCALAR_INV:
+        case ZKP_OP_SCALAR_POW: return 1;
+        default: return ~0u;
+    }
+}
+
+// a resolved view: element i at base + phys(i) * eb
+struct RView {
+    char *base;
+    u64 len, start, whole;  // start = (offset - rotate) mod whole
+    u64 phys(u64 i) const {
+        const u64 p = start + i;
+        return p >= whole ? p - whole : p;
+    }
+    PolyPtr poly() const {
+        // PolyPtr with the same element order: a rotation becomes an offset on the whole array
+        return PolyPtr{reinterpret_cast<u32 *>(base), len, 0, whole ? start : 0, whole ? whole : len};
+    }
+    ConstPolyPtr cpoly() const {
+        return ConstPolyPtr{reinterpret_cast<const u32 *>(base), len, 0, whole ? start : 0, whole ? whole : len};
+    }
+    u32 *ptr() const { return reinterpret_cast<u32 *>(base); }
+};
+
+RView resolve(ZkpServer *s, const Request *r, const ZkpServer::Slot &slot, const ZkpProgView &v) {
+    char *base = nullptr;
+    switch (v.space) {
+        case ZKP_SPACE_DEVICE: base = s->arena.ptr(r->off) + v.addr; break;
+        case ZKP_SPACE_HOST: base = slot.prog_host + v.addr; break;
+        case ZKP_SPACE_ABS: base = reinterpret_cast<char *>(v.addr); break;
+        case ZKP_SPACE_INPUT: base = const_cast<char *>(static_cast<const char *>(r->inputs[v.index])) + v.addr; break;
+        default: break;
+    }
+    RView out{base, v.len, 0, v.whole_len};
+    if (v.whole_len) out.start = (v.offset + v.whole_len - v.rotate % v.whole_len) % v.whole_len;
+    return out;
+}
+
+// element-order copy dst[i] <- src[i], i < len, split where either view wraps (at most 4
+// copies; any direction: the addresses are unified)
+cudaError_t copy_views(const RView &dst, const RView &src, u64 len, u64 eb, cudaStream_t st) {
+    for (u64 i = 0; i < len;) {
+        const u64 sp = src.phys(i), dp = dst.phys(i);
+        const u64 seg = std::min(len - i, std::min(src.whole - sp, dst.whole - dp));
+        cudaError_t e = cudaMemcpyAsync(dst.base + dp * eb, src.base + sp * eb, seg * eb, cudaMemcpyDefault, st);
+        if (e != cudaSuccess) return e;
+        i += seg;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t zero_view(const RView &dst, u64 eb, cudaStream_t st) {
+    for (u64 i = 0; i < dst.len;) {
+        const u64 dp = dst.phys(i);
+        const u64 seg = std::min(dst.len - i, dst.whole - dp);
+        cudaError_t e = cudaMemsetAsync(dst.base + dp * eb, 0, seg * eb, st);
+        if (e != cudaSuccess) return e;
+        i += seg;
+    }
+    return cudaSuccess;
+}
+
+inline u32 log2_exact(u64 n) {
+    u32 l = 0;
+    while ((1ull << l) < n) l++;
+    return l;
+}
+
+// runs the ops of a compiled program in order on the request's stream
+cudaError_t launch_compiled(ZkpServer *s, Request *r, ZkpServer::Slot &slot) {
+    cudaStream_t st = slot.stream;
+    if (r->req.inject_fault == 2) return cudaErrorLaunchFailure;
+    for (const ZkpProgOp &op : r->prog->ops) {
+        RView v[ZKP_PROG_MAX_VIEWS];
+        for (u32 j = 0; j < ZKP_PROG_MAX_VIEWS; j++) v[j] = resolve(s, r, slot, op.v[j]);
+        cudaError_t e = cudaSuccess;
+        switch (op.kind) {
+            case ZKP_OP_COPY:
+                e = copy_views(v[0], v[1], v[0].len, op.imm[0], st);
+                break;
+            case ZKP_OP_ZERO:
+                e = zero_view(v[0], op.imm[0], st);
+                break;
+            case ZKP_OP_NTT:
+                e = op.imm[0] ? zkp_ntt_ex_shoup(v[0].poly(), v[1].ptr(), reinterpret_cast<const u32 *>(op.imm[0]),
+                                                 log2_exact(v[0].len), nullptr, nullptr, st)
+                              : zkp_ntt_ex(v[0].poly(), v[1].ptr(), log2_exact(v[0].len), nullptr, nullptr, st);
+                break;
+            case ZKP_OP_NTT_RECOMPUTE:
+                e = recompute_ntt(v[0].poly(), v[1].ptr(), (u32)op.imm[0], v[2].ptr(), log2_exact(v[0].len), st, 8,
+                                  8);
+                break;
+            case ZKP_OP_DISTRIBUTE:
+                e = distribute_powers(v[0].poly(), v[1].ptr(), v[1].len, st);
+                break;
+            case ZKP_OP_FUSED: {
+                const u32 nv = (u32)op.imm[1], nm = (u32)op.imm[2];
+                // the PolyPtr arrays go through the request's pinned staging to its device
+                // argument buffer, as the reference's wrapper copies them (fused_kernels.rs:165-172)
+                PolyPtr *stage = reinterpret_cast<PolyPtr *>(v[15].base);
+                for (u32 j = 0; j < nv + nm; j++) stage[j] = v[j].poly();
+                e = cudaMemcpyAsync(v[14].base, stage, (nv + nm) * sizeof(PolyPtr), cudaMemcpyHostToDevice, st);
+                if (e == cudaSuccess) {
+                    const PolyPtr *d = reinterpret_cast<const PolyPtr *>(v[14].base);
+                    auto fn = reinterpret_cast<FusedFn>(op.imm[0]);
+                    e = fn(reinterpret_cast<const ConstPolyPtr *>(d), d + nv, op.imm[3], true, nullptr, st);
+                }
+                break;
+            }
+            case ZKP_OP_MSM: {
+                const u32 m = (u32)op.imm[3];
+                const u32 nt = (u32)(op.imm[1] & 0xffffu), w = (u32)(op.imm[1] >> 16);
+                ZkpMsmTask t[32];
+                for (u32 j = 0; j < m; j++)
+                    t[j] = ZkpMsmTask{reinterpret_cast<const u32 *>(op.imm[0]), nt, v[j].ptr(), v[j].len, w,
+                                      v[m + j].ptr(), op.imm[2]};
+                e = zkp_msm_batch(t, m, v[15].base, v[15].len, st);
+                break;
+            }
+            case ZKP_OP_EVAL: {
+                unsigned long tb = (unsigned long)v[0].len;
+                e = poly_eval(v[0].base, &tb, v[2].cpoly(), v[1].ptr(), v[3].ptr(), st);
+                break;
+            }
+            case ZKP_OP_INVERT: {
+                unsigned long tb = (unsigned long)v[0].len;
+                e = batched_invert(v[0].base, &tb, v[1].poly(), st);
+                break;
+            }
+            case ZKP_OP_KATE: {
+                unsigned long tb = (unsigned long)v[0].len;
+                e = kate_division(v[0].base, &tb, log2_exact(v[2].len), v[2].cpoly(), v[3].ptr(), v[1].poly(), st);
+                break;
+            }
+            case ZKP_OP_SCAN: {
+                unsigned long tb = (unsigned long)v[0].len;
+                e = scan_mul(v[0].base, &tb, v[1].poly(), st);
+                break;
+            }
+            case ZKP_OP_ADD: e = poly_add(v[0].poly(), v[1].cpoly(), v[2].cpoly(), st); break;
+            case ZKP_OP_SUB: e = poly_sub(v[0].poly(), v[1].cpoly(), v[2].cpoly(), st); break;
+            case ZKP_OP_ZERO_POLY: e = poly_zero(v[0].poly(), st); break;
+            case ZKP_OP_ONE_LAGRANGE: e = poly_one_lagrange(v[0].poly(), st); break;
+            case ZKP_OP_ONE_COEF: e = poly_one_coef(v[0].poly(), st); break;
+            case ZKP_OP_SCALAR_INV: e = inv_scalar(v[0].ptr(), st); break;
+            case ZKP_OP_SCALAR_POW: e = scalar_pow(v[0].ptr(), op.imm[0], st); break;
+            default: e = cudaErrorInvalidValue; break;
+        }
+        if (e != cudaSuccess) return e;
+    }
+    return cudaEventRecord(slot.done, st);
+}
+
 void finish(ZkpServer *s, Request *r, int status) {
+    if (r->prog) const_cast<ZkpProgram *>(r->prog)->live--;
     r->res.status = status;
     r->res.done_s = s->now();
     r->done = true;
@@ -288,8 +503,14 @@ void worker_loop(ZkpServer *s) {
             if (q == cudaErrorNotReady) continue;
             Request *r = slot.req;
             if (q == cudaSuccess) {
-                memcpy(r->res.msm, slot.host, sizeof(r->res.msm));
-                memcpy(r->res.evals, slot.host + 64, sizeof(r->res.evals));
+                if (r->prog) {
+                    for (const ZkpProgOut &o : r->prog->outs)
+                        memcpy(static_cast<char *>(r->results) + o.result_offset, slot.prog_host + o.host_offset,
+                               o.bytes);
+                } else {
+                    memcpy(r->res.msm, slot.host, sizeof(r->res.msm));
+                    memcpy(r->res.evals, slot.host + 64, sizeof(r->res.evals));
+                }
                 finish(s, r, 0);
             } else {
                 finish(s, r, -3);
@@ -331,7 +552,16 @@ void worker_loop(ZkpServer *s) {
             s->inflight++;
             s->stats.peak_inflight = std::max<u64>(s->stats.peak_inflight, s->inflight);
             s->stats.peak_bytes = s->arena.peak();
-            cudaError_t e = launch_program(s, r, slot);
+            cudaError_t e = cudaSuccess;
+            if (r->prog && slot.prog_host_bytes < r->prog->host_bytes) {
+                // the slot is idle (its last request completed), so its host block can grow
+                if (slot.prog_host) cudaFreeHost(slot.prog_host);
+                slot.prog_host = nullptr;
+                slot.prog_host_bytes = 0;
+                e = cudaMallocHost(reinterpret_cast<void **>(&slot.prog_host), r->prog->host_bytes);
+                if (e == cudaSuccess) slot.prog_host_bytes = r->prog->host_bytes;
+            }
+            if (e == cudaSuccess) e = r->prog ? launch_compiled(s, r, slot) : launch_program(s, r, slot);
             if (e != cudaSuccess) {
                 // the request fails alone: drain what was queued on its stream, release it
                 cudaStreamSynchronize(slot.stream);
@@ -529,6 +759,7 @@ extern "C" void zkp_serve_destroy(ZkpServer *s) {
         if (slot.stream) cudaStreamDestroy(slot.stream);
         if (slot.done) cudaEventDestroy(slot.done);
         if (slot.host) cudaFreeHost(slot.host);
+        if (slot.prog_host) cudaFreeHost(slot.prog_host);
     }
     for (auto &c : s->consts) {
         cudaFree(c.inv_tw);
@@ -542,4 +773,103 @@ extern "C" void zkp_serve_destroy(ZkpServer *s) {
     for (auto &kv : s->all) delete kv.second;
     if (s->fused_lib) dlclose(s->fused_lib);
     delete s;
+}
+
+// ------------------------------------------------------------------ compiled programs
+extern "C" cudaError_t zkp_serve_program_create(ZkpServer *s, const ZkpProgOp *ops, unsigned int n_ops,
+                                                unsigned long long device_bytes, unsigned long long host_bytes,
+                                                const ZkpProgOut *outs, unsigned int n_outs,
+                                                const unsigned long long *input_bytes, unsigned int n_inputs,
+                                                ZkpProgram **out) {
+    if (!s || !out || (n_ops && !ops) || (n_outs && !outs) || (n_inputs && !input_bytes))
+        return cudaErrorInvalidValue;
+    for (unsigned i = 0; i < n_ops; i++) {
+        const ZkpProgOp &op = ops[i];
+        const u32 need = required_views(op);
+        if (need == ~0u || op.n_views > ZKP_PROG_MAX_VIEWS || need > op.n_views) return cudaErrorInvalidValue;
+        if (op.kind == ZKP_OP_FUSED && (op.imm[0] == 0 || op.imm[1] + op.imm[2] > 14 || op.imm[3] == 0))
+            return cudaErrorInvalidValue;
+        if (op.kind == ZKP_OP_MSM && (op.imm[0] == 0 || op.imm[3] == 0 || op.imm[3] > 7)) return cudaErrorInvalidValue;
+        if ((op.kind == ZKP_OP_COPY || op.kind == ZKP_OP_ZERO) && op.imm[0] != 32 && op.imm[0] != 64)
+            return cudaErrorInvalidValue;
+        if (op.kind == ZKP_OP_COPY && op.v[0].len != op.v[1].len) return cudaErrorInvalidValue;
+        for (u32 j = 0; j < ZKP_PROG_MAX_VIEWS; j++) {
+            const ZkpProgView &v = op.v[j];
+            if (v.space == ZKP_SPACE_NONE) continue;
+            if (!view_well_formed(v)) return cudaErrorInvalidValue;
+            const u64 end = v.addr + v.whole_len * view_elem_bytes(op, j);
+            if (v.space == ZKP_SPACE_DEVICE && end > device_bytes) return cudaErrorInvalidValue;
+            if (v.space == ZKP_SPACE_HOST && end > host_bytes) return cudaErrorInvalidValue;
+            if (v.space == ZKP_SPACE_INPUT && (v.index >= n_inputs || end > input_bytes[v.index]))
+                return cudaErrorInvalidValue;
+            if (v.space > ZKP_SPACE_INPUT) return cudaErrorInvalidValue;
+        }
+        // the fused argument buffer and its staging, the MSM workspace: present and large enough
+        if (op.kind == ZKP_OP_FUSED) {
+            const u64 bytes = (op.imm[1] + op.imm[2]) * sizeof(PolyPtr);
+            if (op.v[14].space != ZKP_SPACE_DEVICE || op.v[14].len < bytes || op.v[15].space != ZKP_SPACE_HOST ||
+                op.v[15].len < bytes)
+                return cudaErrorInvalidValue;
+        }
+        if (op.kind == ZKP_OP_MSM && op.v[15].space != ZKP_SPACE_DEVICE) return cudaErrorInvalidValue;
+    }
+    u64 extent = 0;
+    for (unsigned i = 0; i < n_outs; i++) {
+        if (outs[i].host_offset + outs[i].bytes > host_bytes) return cudaErrorInvalidValue;
+        extent = std::max<u64>(extent, outs[i].result_offset + outs[i].bytes);
+    }
+    auto *p = new ZkpProgram();
+    p->ops.assign(ops, ops + n_ops);
+    p->device_bytes = std::max<u64>(device_bytes, 256);
+    p->host_bytes = std::max<u64>(host_bytes, 256);
+    p->outs.assign(outs, outs + n_outs);
+    p->result_extent = extent;
+    p->input_bytes.assign(input_bytes, input_bytes + n_inputs);
+    *out = p;
+    return cudaSuccess;
+}
+
+extern "C" long long zkp_serve_submit_program(ZkpServer *s, const ZkpProgram *prog, const void *const *inputs,
+                                              unsigned int n_inputs, void *results,
+                                              unsigned long long results_bytes) {
+    if (!s || !prog) return -1;
+    auto *r = new Request();
+    memset(&r->req, 0, sizeof(r->req));
+    memset(&r->res, 0, sizeof(r->res));
+    r->prog = prog;
+    const_cast<ZkpProgram *>(prog)->live++;
+    std::lock_guard<std::mutex> g(s->mu);
+    if (s->stop) {
+        const_cast<ZkpProgram *>(prog)->live--;
+        delete r;
+        return -1;
+    }
+    r->ticket = s->next_ticket++;
+    r->res.submit_s = s->now();
+    s->all[r->ticket] = r;
+    bool ok = n_inputs == prog->input_bytes.size() && (n_inputs == 0 || inputs != nullptr) &&
+              results_bytes >= prog->result_extent && (prog->result_extent == 0 || results != nullptr);
+    for (unsigned i = 0; ok && i < n_inputs; i++) ok = inputs[i] != nullptr || prog->input_bytes[i] == 0;
+    if (!ok) {
+        finish(s, r, -1);
+        s->cv_done.notify_all();
+        return r->ticket;
+    }
+    r->inputs.assign(inputs, inputs + n_inputs);
+    r->results = results;
+    r->bytes = prog->device_bytes;
+    r->res.footprint = prog->device_bytes;
+    if (al(prog->device_bytes) > s->arena.size()) {
+        finish(s, r, -2);
+        s->cv_done.notify_all();
+        return r->ticket;
+    }
+    s->pending.push_back(r);
+    s->cv_work.notify_one();
+    return r->ticket;
+}
+
+extern "C" void zkp_serve_program_destroy(ZkpServer *s, ZkpProgram *prog) {
+    (void)s;
+    delete prog;
 }

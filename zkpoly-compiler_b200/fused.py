@@ -348,5 +348,10 @@ def quotient_kernel() -> FusedKernel:
 
 
 def build_path_kernels() -> list[str]:
-    """Builds the fused kernels the hot path uses (called by the package build)."""
-    return [FusedOp(quotient_graph(), "zkp_quotient_z8").build()]
+    """Builds the fused kernels the hot path uses (called by the package build): the quotient
+    kernel of the built-in served program and the two kernels its compiled-artifact form
+    names (program.prover_fused_graphs)."""
+    from .program import prover_fused_graphs
+    out = [FusedOp(quotient_graph(), "zkp_quotient_z8").build()]
+    out += [FusedOp(g, name).build() for name, g in prover_fused_graphs().items()]
+    return out

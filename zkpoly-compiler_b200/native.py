@@ -45,6 +45,7 @@ SIGNATURES = {
         "zkp_coset_lde": (cudaError_t, [PolyPtr, PolyPtr, c_void_p, ctypes.c_uint, ctypes.c_uint, c_void_p,
                                         c_void_p]),
         "zkp_ntt_shoup_table": (cudaError_t, [c_void_p, ctypes.c_uint, c_void_p, c_void_p]),
+        "zkp_ntt_roots_device": (cudaError_t, [c_void_p, ctypes.c_ulonglong, c_void_p, c_void_p]),
         "zkp_ntt_shoup_probe": (cudaError_t, [ctypes.c_uint, ctypes.c_uint, c_void_p, c_void_p]),
         "zkp_ntt_ex_shoup": (cudaError_t, [PolyPtr, c_void_p, c_void_p, ctypes.c_uint, c_void_p, c_void_p, c_void_p]),
         "zkp_coset_lde_shoup": (cudaError_t, [PolyPtr, PolyPtr, c_void_p, c_void_p, ctypes.c_uint, ctypes.c_uint,
@@ -105,6 +106,12 @@ SIGNATURES = {
         "zkp_serve_stats": (None, [c_void_p, c_void_p]),
         "zkp_serve_now": (ctypes.c_double, [c_void_p]),
         "zkp_serve_destroy": (None, [c_void_p]),
+        "zkp_serve_program_create": (cudaError_t, [c_void_p, c_void_p, ctypes.c_uint, ctypes.c_ulonglong,
+                                                   ctypes.c_ulonglong, c_void_p, ctypes.c_uint, c_void_p,
+                                                   ctypes.c_uint, ctypes.POINTER(c_void_p)]),
+        "zkp_serve_submit_program": (ctypes.c_longlong, [c_void_p, c_void_p, c_void_p, ctypes.c_uint, c_void_p,
+                                                         ctypes.c_ulonglong]),
+        "zkp_serve_program_destroy": (None, [c_void_p, c_void_p]),
     },
     "libpoly.so": {
         "poly_add": (cudaError_t, [PolyPtr, PolyPtr, PolyPtr, c_void_p]),
@@ -163,6 +170,26 @@ class ZkpProverResult(ctypes.Structure):
     _fields_ = [("status", ctypes.c_int), ("msm", (ctypes.c_uint * 16) * 4), ("evals", (ctypes.c_uint * 8) * 2),
                 ("submit_s", ctypes.c_double), ("start_s", ctypes.c_double), ("done_s", ctypes.c_double),
                 ("footprint", ctypes.c_ulonglong)]
+
+
+ZKP_PROG_MAX_VIEWS = 16
+
+
+class ZkpProgView(ctypes.Structure):
+    """include/zkp_runtime.h: one operand of a lowered program op."""
+    _fields_ = [("space", ctypes.c_uint), ("index", ctypes.c_uint), ("addr", ctypes.c_ulonglong),
+                ("len", ctypes.c_ulonglong), ("rotate", ctypes.c_ulonglong), ("offset", ctypes.c_ulonglong),
+                ("whole_len", ctypes.c_ulonglong)]
+
+
+class ZkpProgOp(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_uint), ("n_views", ctypes.c_uint), ("imm", ctypes.c_ulonglong * 4),
+                ("v", ZkpProgView * ZKP_PROG_MAX_VIEWS)]
+
+
+class ZkpProgOut(ctypes.Structure):
+    _fields_ = [("host_offset", ctypes.c_ulonglong), ("bytes", ctypes.c_ulonglong),
+                ("result_offset", ctypes.c_ulonglong)]
 
 
 class ZkpServeStats(ctypes.Structure):
