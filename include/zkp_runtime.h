@@ -89,6 +89,19 @@ unsigned long long zkp_serve_footprint(const ZkpServer *s, unsigned int k);
 /* Blocks until the ticket completes or timeout_s elapses: returns 0 when done, 1 on timeout. */
 int zkp_serve_wait(ZkpServer *s, long long ticket, ZkpProverResult *out, double timeout_s);
 void zkp_serve_stats(const ZkpServer *s, ZkpServeStats *out);
+/* Admission policy for the latency tail of a mixed-size load, which is made of its largest
+ * requests (all fields 0 = the default: one priority, no class limit).  Requests whose planned
+ * footprint is at least priority_bytes run on their slot's high-priority stream, so their
+ * blocks are scheduled ahead of those of requests admitted around them; at most
+ * max_large_inflight requests of at least large_bytes run at once (smaller requests are
+ * admitted past a waiting large one, within the look-ahead).  Applies to admissions from now
+ * on. */
+typedef struct ZkpServePolicy {
+    unsigned long long priority_bytes;
+    unsigned long long large_bytes;
+    unsigned int max_large_inflight;
+} ZkpServePolicy;
+void zkp_serve_set_policy(ZkpServer *s, const ZkpServePolicy *policy);
 double zkp_serve_now(const ZkpServer *s);
 void zkp_serve_destroy(ZkpServer *s);
 

@@ -46,6 +46,15 @@ def test_mixed_workload_batched_equals_plain(zk, orc):
     assert all(torch.equal(a, b) for a, b in zip(plain_ntt, ref_ntt))
     for a, b in zip(ref_msm, plain_msm):
         assert np.array_equal(a, b.cpu().numpy().view(np.uint32))
+    # the per-call path over the batch's own resident tables and Shoup twiddle tables agrees
+    w.reset_inputs()
+    for r in w.results:
+        r.zero_()
+    w.run_plain_same_tables()
+    torch.cuda.synchronize()
+    same_ntt, same_msm = w.snapshot()
+    assert all(torch.equal(a, b) for a, b in zip(plain_ntt, same_ntt))
+    assert all(torch.equal(a, b) for a, b in zip(plain_msm, same_msm))
     # replay again: same results
     w.reset_inputs()
     w.run_batched()

@@ -1,4 +1,6 @@
 """Generated fused kernels and the fused quotient pipeline on the GPU, bit-exact vs the oracle."""
+import os
+
 import numpy as np
 import pytest
 import torch
@@ -232,3 +234,47 @@ def test_fixed_factor_products(zk, orc):
            orc.vec_mul(a, qf)]
     for o, e in zip(outs, exp):
         assert np.array_equal(o.numpy_u64(), e)
+
+
+def _arith_graph(repr_):
+    import json
+    from conftest import GOLDEN
+    with open(os.path.join(GOLDEN, "arith_graph_coef.json")) as f:
+        g = json.load(f)
+    g["poly_repr"] = repr_
+    return g
+
+
+@pytest.mark.parametrize("repr_", ["Coef", "Lagrange"])
+def test_kernel_from_reference_arith_graph(zk, orc, repr_):
+    """A fused kernel generated from a serialised ArithGraph (the reference fusion pass's output):
+    Pp / Ss / Sp ops, neg, pow, an in-place input and a scalar output, against the oracle; on a
+    Coef graph the Sp add / sub / sub-by apply at index 0 only (kernel_gen.rs:501-545)."""
+    n = 1000
+    graph = zk.fused.FusedGraph.from_arith_graph(_arith_graph(repr_))
+    kern = zk.fused.FusedKernel(zk.fused.FusedOp(graph))
+    a, b, acc = (orc.gen_fr(s, n) for s in (71, 72, 73))
+    s_, t = orc.gen_fr(74, 1)[0], orc.gen_fr(75, 1)[0]
+    dev_acc = dev(zk, acc)
+    scal = torch.zeros((1, 8), dtype=torch.int32, device="cuda")
+    out2 = zk.ScalarArray.zeros(n)
+    kern([dev_acc, scal, out2], [dev(zk, a), dev(zk, b), zk.ScalarArray.from_numpy(s_[None, :]).values,
+                                 zk.ScalarArray.from_numpy(t[None, :]).values])
+    torch.cuda.synchronize()
+    S, T = np.tile(s_, (n, 1)), np.tile(t, (n, 1))
+    coef = repr_ == "Coef"
+    ab = orc.vec_mul(a, b)
+    v6 = ab.copy()
+    v6[: 1 if coef else n] = orc.vec_add(S, ab)[: 1 if coef else n]
+    st = orc.mul(s_, t)
+    v8 = v6.copy()
+    v8[: 1 if coef else n] = orc.vec_sub(v6, np.tile(st, (n, 1)))[: 1 if coef else n]
+    v9 = orc.vec_sub(np.zeros_like(v8), v8)
+    v10 = orc.vec_mul(orc.vec_mul(a, a), a)
+    v12 = orc.vec_add(orc.vec_sub(v9, v10), acc)
+    v13 = orc.vec_sub(np.zeros_like(b), b)
+    v13[: 1 if coef else n] = orc.vec_sub(T, b)[: 1 if coef else n]
+    v15 = orc.vec_add(v12, orc.vec_mul(T, v13))
+    assert np.array_equal(dev_acc.numpy_u64(), v15)
+    assert np.array_equal(scal.cpu().numpy().view(np.uint64).reshape(4), orc.sub(s_, t))
+    assert np.array_equal(out2.numpy_u64(), v9)

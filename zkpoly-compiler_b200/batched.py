@@ -9,6 +9,9 @@ plain (reference ABI): the per-call path as the reference's runtime drives it - 
          MSM with host scalars and a host point table (core/src/msm.rs:302-369), in order.
 plain (device): the same per-call order, but each MSM is zkp_msm_device over device-resident
          bases (one table) - the per-call path with the host copies taken out.
+plain (same tables): the per-call order with everything the batch has except the batching:
+         each transform through its own zkp_ntt_ex_shoup call (Shoup twiddle tables), each MSM
+         a batch of one over the same resident precomputed table sets the batch reads.
 batched: one NttBatch plan (a persistent launch per pass shared by every transform) on one
          stream and MsmBatch launches (every stage shared by up to 32 MSMs) over precomputed
          resident tables on a second stream, captured once into a CUDA graph and replayed.
@@ -67,6 +70,32 @@ class MixedWorkload:
             check(lib.zkp_msm_device(self.ws.data_ptr(), self.ws.numel(), self.bases.data_ptr(), 1, s.data_ptr(),
                                      1 << L, w, r.data_ptr(), torch.cuda.current_stream().cuda_stream
                                      if stream is None else stream.cuda_stream), "zkp_msm_device")
+
+    # ---- per-call path over the batch's own tables
+    def build_plain_same_tables(self):
+        if self.tables is None:
+            self._resident_tables()
+        self.single = []
+        for s, L, r in zip(self.scalars, self.msm_logs, self.results):
+            c, nt = tuner.msm_resident_config(1 << L)
+            t, rows = self.tables[(c, nt)]
+            self.single.append(msm.MsmBatch([{"points": t, "n_tables": nt, "table_stride": rows, "scalars": s,
+                                               "n": 1 << L, "window": c, "result": r}]))
+
+    def run_plain_same_tables(self, stream=None):
+        if not hasattr(self, "single"):
+            self.build_plain_same_tables()
+        for x, L, kind in zip(self.ntt_bufs, self.ntt_logs, self.ntt_kinds):
+            inv = kind == "intt"
+            tw, sh = ntt.twiddle_table(L, inv), ntt.shoup_table(L, inv)
+            if kind == "ntt":
+                ntt.ntt_ex(x, tw, None, None, stream, shoup=sh)
+            elif kind == "intt":
+                ntt.ntt_ex(x, tw, None, ntt.n_inv(L), stream, shoup=sh)
+            else:
+                ntt.ntt_ex(x, tw, ntt.scalar_const(7), None, stream, shoup=sh)
+        for b in self.single:
+            b.run(stream)
 
     # ---- per-call path through the reference ABI (host arrays for the MSMs)
     def run_plain_ref_abi(self, stream=None):

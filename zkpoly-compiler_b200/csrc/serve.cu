@@ -120,6 +120,8 @@ struct Request {
     size_t off = SIZE_MAX, bytes = 0;
     int slot = -1;
     bool done = false;
+    cudaStream_t stream = nullptr;  // the slot's stream of the request's priority class
+    bool large = false;             // counted against the policy's large-request limit
     // a request of a compiled program (null for the built-in prover program)
     const ZkpProgram *prog = nullptr;
     std::vector<const void *> inputs;
@@ -155,7 +157,8 @@ struct ZkpServer {
     FusedFn fused = nullptr;
 
     struct Slot {
-        cudaStream_t stream = nullptr;
+        cudaStream_t stream = nullptr;     // normal priority
+        cudaStream_t stream_hi = nullptr;  // high priority (requests of at least priority_bytes)
         cudaEvent_t done = nullptr;
         u32 *host = nullptr;    // pinned: results (4*16 + 2*8 words) + PolyPtr staging
         char *prog_host = nullptr;  // pinned host block of compiled-program requests
@@ -174,6 +177,8 @@ struct ZkpServer {
     std::chrono::steady_clock::time_point t0;
     ZkpServeStats stats{};
     u64 inflight = 0;
+    ZkpServePolicy policy{};  // priorities and the large-request limit (all 0: off)
+    u64 large_inflight = 0;
 
     double now() const {
         return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -227,7 +232,7 @@ cudaError_t launch_program(ZkpServer *s, Request *r, ZkpServer::Slot &slot) {
     plan_request(s, k, &p);
     char *base = s->arena.ptr(r->off);
     auto P = [&](size_t off) { return reinterpret_cast<u32 *>(base + off); };
-    cudaStream_t st = slot.stream;
+    cudaStream_t st = r->stream;
     const SizeConsts &sc = s->consts[k];
     const u64 seed = r->req.seed * 8;
 #define RUN(x)                                   \
@@ -397,7 +402,7 @@ inline u32 log2_exact(u64 n) {
 
 // runs the ops of a compiled program in order on the request's stream
 cudaError_t launch_compiled(ZkpServer *s, Request *r, ZkpServer::Slot &slot) {
-    cudaStream_t st = slot.stream;
+    cudaStream_t st = r->stream;
     if (r->req.inject_fault == 2) return cudaErrorLaunchFailure;
     for (const ZkpProgOp &op : r->prog->ops) {
         RView v[ZKP_PROG_MAX_VIEWS];
@@ -491,6 +496,13 @@ void finish(ZkpServer *s, Request *r, int status) {
         s->stats.failed++;
 }
 
+// a request of the class the policy limits; the class is fixed at admission (r->large)
+bool is_large(const ZkpServer *s, Request *r) {
+    if (r->slot < 0) r->large = s->policy.max_large_inflight && s->policy.large_bytes &&
+                                r->bytes >= s->policy.large_bytes;
+    return r->large;
+}
+
 void worker_loop(ZkpServer *s) {
     cudaSetDevice(s->device);
     std::unique_lock<std::mutex> lk(s->mu);
@@ -516,6 +528,7 @@ void worker_loop(ZkpServer *s) {
                 finish(s, r, -3);
             }
             s->arena.release(r->off, r->bytes);
+            if (is_large(s, r)) s->large_inflight--;
             slot.req = nullptr;
             s->inflight--;
             progressed = true;
@@ -538,6 +551,10 @@ void worker_loop(ZkpServer *s) {
                 s->cv_done.notify_all();
                 continue;
             }
+            if (is_large(s, r) && s->large_inflight >= s->policy.max_large_inflight) {
+                idx++;  // a large request waits for another to finish; smaller ones may pass
+                continue;
+            }
             size_t off = s->arena.alloc(r->bytes);
             if (off == SIZE_MAX) {
                 idx++;
@@ -549,6 +566,12 @@ void worker_loop(ZkpServer *s) {
             r->res.start_s = s->now();
             auto &slot = s->slots[free_slot];
             slot.req = r;
+            // large requests make up the latency tail: with the policy's priority_bytes set they
+            // run on the slot's high-priority stream, so the blocks of requests admitted around
+            // them queue behind theirs instead of sharing the SMs evenly
+            r->stream = (s->policy.priority_bytes && r->bytes >= s->policy.priority_bytes) ? slot.stream_hi
+                                                                                               : slot.stream;
+            if (is_large(s, r)) s->large_inflight++;
             s->inflight++;
             s->stats.peak_inflight = std::max<u64>(s->stats.peak_inflight, s->inflight);
             s->stats.peak_bytes = s->arena.peak();
@@ -564,9 +587,10 @@ void worker_loop(ZkpServer *s) {
             if (e == cudaSuccess) e = r->prog ? launch_compiled(s, r, slot) : launch_program(s, r, slot);
             if (e != cudaSuccess) {
                 // the request fails alone: drain what was queued on its stream, release it
-                cudaStreamSynchronize(slot.stream);
+                cudaStreamSynchronize(r->stream);
                 cudaGetLastError();
                 s->arena.release(r->off, r->bytes);
+                if (is_large(s, r)) s->large_inflight--;
                 slot.req = nullptr;
                 s->inflight--;
                 finish(s, r, -3);
@@ -678,9 +702,12 @@ extern "C" cudaError_t zkp_serve_create(const ZkpServeConfig *cfg, const unsigne
         if (e == cudaSuccess) e = cudaMemcpy(c.zh_inv, zh.data(), (32u << ext), cudaMemcpyHostToDevice);
     }
     if (tmp) cudaFree(tmp);
+    int prio_low = 0, prio_high = 0;
+    if (e == cudaSuccess) e = cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
     s->slots.resize(cfg->max_inflight);
     for (auto &slot : s->slots) {
-        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&slot.stream, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&slot.stream, cudaStreamNonBlocking, prio_low);
+        if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&slot.stream_hi, cudaStreamNonBlocking, prio_high);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&slot.done, cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaMallocHost(&slot.host, 4096);
     }
@@ -747,6 +774,12 @@ extern "C" void zkp_serve_stats(const ZkpServer *s, ZkpServeStats *out) {
 
 extern "C" double zkp_serve_now(const ZkpServer *s) { return s->now(); }
 
+extern "C" void zkp_serve_set_policy(ZkpServer *s, const ZkpServePolicy *policy) {
+    if (!s || !policy) return;
+    std::lock_guard<std::mutex> g(s->mu);
+    s->policy = *policy;
+}
+
 extern "C" void zkp_serve_destroy(ZkpServer *s) {
     if (!s) return;
     {
@@ -757,6 +790,7 @@ extern "C" void zkp_serve_destroy(ZkpServer *s) {
     if (s->worker.joinable()) s->worker.join();
     for (auto &slot : s->slots) {
         if (slot.stream) cudaStreamDestroy(slot.stream);
+        if (slot.stream_hi) cudaStreamDestroy(slot.stream_hi);
         if (slot.done) cudaEventDestroy(slot.done);
         if (slot.host) cudaFreeHost(slot.host);
         if (slot.prog_host) cudaFreeHost(slot.prog_host);

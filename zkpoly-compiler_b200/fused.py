@@ -64,6 +64,99 @@ class FusedGraph:
     def key(self) -> str:
         return hashlib.sha1(repr((self.nodes, self.coef)).encode()).hexdigest()[:16]
 
+    @staticmethod
+    def from_arith_graph(g: dict) -> "FusedGraph":
+        """The node list of a serialised ArithGraph, the fusion pass's output that the
+        reference's generator consumes (common/src/arith.rs:323-330; kernel_gen.rs:47-121).
+
+        serde forms: ``{"outputs": [ids], "inputs": [ids], "g": [[vertex, ...], null],
+        "poly_repr": "Coef" | "Lagrange", "poly_degree": n | null}`` with a vertex
+        ``{"op": {"Input": {"outer_id", "typ": "Scalar" | "ScalarArray", "mutability": "Const" |
+        "Mut"}}}``, ``{"op": {"Arith": {"Bin": [{"Pp" | "Ss" | "Sp": op}, lhs, rhs]}}}``,
+        ``{"op": {"Arith": {"Unr": [{"P" | "S": "Neg" | {"Pow": e}}, x]}}}`` or ``{"op":
+        {"Output": {"outer_id", "typ", "store_node", "in_node"}}}``.  Argument order follows
+        ArithGraph::gen_var_lists (arith.rs:429-455): mut_vars are the outputs in order; vars
+        are the inputs in order except in-place ones (a Mut input that is some output's
+        in_node, arith.rs:411-427), which are read from that output's mut_vars slot
+        (kernel_gen.rs:53-79).  An Sp op's lhs is the scalar and rhs the polynomial; on a Coef
+        graph Sp add / sub / sub-by touch index 0 only (kernel_gen.rs:501-545).  Division,
+        inversion and scalar powers are not fused (the reference rejects them as well)."""
+        verts = g["g"][0] if isinstance(g["g"], list) and len(g["g"]) == 2 and g["g"][1] is None else g["g"]
+        ops = [v["op"] if isinstance(v, dict) and "op" in v else v for v in verts]
+        kind_of = {}
+        for i, op in enumerate(ops):
+            if op == "Todo" or not isinstance(op, dict) or len(op) != 1:
+                raise ValueError(f"vertex {i}: unsupported operation {op!r:.80}")
+            kind_of[i] = next(iter(op))
+        inplace = {}
+        for m, oid in enumerate(g["outputs"]):
+            out = ops[oid].get("Output")
+            if out is None:
+                raise ValueError(f"output {oid} is not an Output vertex")
+            src = out.get("in_node")
+            if src is not None and ops[src]["Input"]["mutability"] == "Mut":
+                inplace[src] = m
+        var_index = {}
+        for iid in g["inputs"]:
+            if "Input" not in ops[iid]:
+                raise ValueError(f"input {iid} is not an Input vertex")
+            if iid not in inplace:
+                var_index[iid] = len(var_index)
+
+        def deps(i):
+            op = ops[i]
+            if "Arith" in op:
+                a = op["Arith"]
+                return a["Bin"][1:] if "Bin" in a else [a["Unr"][1]]
+            if "Output" in op:
+                return [op["Output"]["store_node"]]
+            return []
+        order, state = [], {}
+
+        def visit(i):
+            if state.get(i) == 2:
+                return
+            if state.get(i) == 1:
+                raise ValueError("the arithmetic graph has a cycle")
+            state[i] = 1
+            for d in deps(i):
+                visit(int(d))
+            state[i] = 2
+            order.append(i)
+        for i in list(g["inputs"]) + list(g["outputs"]):
+            visit(int(i))
+        nodes = []
+        bin_names = {"Add": "add", "Sub": "sub", "Mul": "mul"}
+        for i in order:
+            op, name = ops[i], f"v{i}"
+            if "Input" in op:
+                kind = "scalar" if op["Input"]["typ"] == "Scalar" else "poly"
+                side, idx = ("mut", inplace[i]) if i in inplace else ("var", var_index[i])
+                nodes.append(("input", name, kind, side, idx))
+            elif "Output" in op:
+                m = list(g["outputs"]).index(i)
+                nodes.append(("output", m, f"v{op['Output']['store_node']}"))
+            elif "Bin" in op["Arith"]:
+                (cls, bop), lhs, rhs = next(iter(op["Arith"]["Bin"][0].items())), *op["Arith"]["Bin"][1:]
+                if cls in ("Pp", "Ss"):
+                    if bop not in bin_names:
+                        raise ValueError(f"vertex {i}: {cls} {bop} is not fused (batched inversion handles it)")
+                    nodes.append((bin_names[bop], name, f"v{lhs}", f"v{rhs}"))
+                else:
+                    sp = {"Add": "sp_add", "Sub": "sp_sub", "SubBy": "sp_subby", "Mul": "mul"}.get(bop)
+                    if sp is None:
+                        raise ValueError(f"vertex {i}: Sp {bop} is not fused (batched inversion handles it)")
+                    nodes.append((sp, name, f"v{lhs}", f"v{rhs}"))
+            else:
+                (cls, uop), x = next(iter(op["Arith"]["Unr"][0].items())), op["Arith"]["Unr"][1]
+                if uop == "Neg":
+                    nodes.append(("neg", name, f"v{x}"))
+                elif isinstance(uop, dict) and "Pow" in uop and cls == "P":
+                    nodes.append(("pow", name, f"v{x}", int(uop["Pow"])))
+                else:
+                    raise ValueError(f"vertex {i}: {cls} {uop!r} is not fused")
+        return FusedGraph(nodes, coef=g.get("poly_repr") == "Coef")
+
 
 class FusedOp:
     """Generates and builds one fused kernel (kernel_gen.rs FusedOp::new / gen)."""

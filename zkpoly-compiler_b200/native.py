@@ -105,6 +105,7 @@ SIGNATURES = {
         "zkp_serve_wait": (ctypes.c_int, [c_void_p, ctypes.c_longlong, c_void_p, ctypes.c_double]),
         "zkp_serve_stats": (None, [c_void_p, c_void_p]),
         "zkp_serve_now": (ctypes.c_double, [c_void_p]),
+        "zkp_serve_set_policy": (None, [c_void_p, c_void_p]),
         "zkp_serve_destroy": (None, [c_void_p]),
         "zkp_serve_program_create": (cudaError_t, [c_void_p, c_void_p, ctypes.c_uint, ctypes.c_ulonglong,
                                                    ctypes.c_ulonglong, c_void_p, ctypes.c_uint, c_void_p,
@@ -190,6 +191,11 @@ class ZkpProgOp(ctypes.Structure):
 class ZkpProgOut(ctypes.Structure):
     _fields_ = [("host_offset", ctypes.c_ulonglong), ("bytes", ctypes.c_ulonglong),
                 ("result_offset", ctypes.c_ulonglong)]
+
+
+class ZkpServePolicy(ctypes.Structure):
+    _fields_ = [("priority_bytes", ctypes.c_ulonglong), ("large_bytes", ctypes.c_ulonglong),
+                ("max_large_inflight", ctypes.c_uint)]
 
 
 class ZkpServeStats(ctypes.Structure):

@@ -645,9 +645,7 @@ def resident_table(table: list, gpu_mapping=None) -> list:
         if art.binary_size(c.typ) is None:
             out.append(c)
             continue
-        words = art._value_tensor(c)
-        dev = art.torch_device(c.device, gpu_mapping)
-        words = words.to(dev) if dev.type == "cuda" else words.clone()
+        words = art._value_tensor(c).to(art.torch_device(c.device, gpu_mapping), copy=True)
         out.append(art.Constant(c.name, c.typ, c.device, art._wrap(c.typ, words)))
     return out
 
@@ -779,15 +777,15 @@ def prover_input_types(k: int, ext: int = 2) -> list:
 
 
 def prover_constants(k: int, ext: int = 2, points=None) -> dict:
-    """The prover program's constants computed on the device by this package (uint32 host
+    """The prover program's constants, computed by this package (device tensors, small host
     arrays): inverse roots of 2^k, forward roots of 2^(k+ext) (the ssip_precompute tables),
     n^-1, the coset powers 7^i (i < 2^k), 1/Z_H at the 2^ext coset classes, and the first 2^k
     rows of ``points`` ((rows, 16) int32 device tensor) as the bases."""
     from . import ntt, pipeline
     from .field import FR_MODULUS, GENERATOR, mont_words
     n = 1 << k
-    out = {"inv_twiddle": ntt.twiddle_table(k, True).values.cpu().numpy().view(np.uint32),
-           "fwd_twiddle": ntt.twiddle_table(k + ext, False).values.cpu().numpy().view(np.uint32),
+    out = {"inv_twiddle": ntt.twiddle_table(k, True).values,
+           "fwd_twiddle": ntt.twiddle_table(k + ext, False).values,
            "n_inv": mont_words(pow(n, -1, FR_MODULUS)).reshape(1, 8),
            "zh_inv": np.stack([mont_words(v) for v in pipeline.zh_inv_values(k, ext)])}
     g = mont_words(GENERATOR)
@@ -796,9 +794,9 @@ def prover_constants(k: int, ext: int = 2, points=None) -> dict:
     unit = torch.from_numpy(g.view(np.int32).copy()).cuda()
     check(load("libntt.so").zkp_ntt_roots_device(powers.data_ptr(), n, unit.data_ptr(), None),
           "zkp_ntt_roots_device")
-    out["coset_powers"] = powers.cpu().numpy().view(np.uint32)
+    out["coset_powers"] = powers
     if points is not None:
-        out["bases"] = points[:n].cpu().numpy().view(np.uint32).reshape(n, 16)
+        out["bases"] = points[:n]
     torch.cuda.synchronize()
     return out
 

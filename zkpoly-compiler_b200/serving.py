@@ -42,6 +42,16 @@ class Server:
         self.h = ctypes.c_void_p()
         check(self.lib.zkp_serve_create(ctypes.byref(cfg), ptr, n_bases, ctypes.byref(self.h)), "zkp_serve_create")
 
+    def set_policy(self, priority_k: int = 0, large_k: int = 0, max_large_inflight: int = 0) -> None:
+        """zkp_serve_set_policy with its thresholds given as sizes: requests at least as large
+        (by planned footprint) as a built-in request of size priority_k run on high-priority
+        streams; at most max_large_inflight requests at least as large as one of size large_k
+        run at once.  Zeros turn each off."""
+        from .native import ZkpServePolicy
+        fp = lambda k: int(self.lib.zkp_serve_footprint(self.h, k)) if k else 0  # noqa: E731
+        pol = ZkpServePolicy(fp(priority_k), fp(large_k), max_large_inflight)
+        self.lib.zkp_serve_set_policy(self.h, ctypes.byref(pol))
+
     def footprint(self, k: int) -> int:
         return int(self.lib.zkp_serve_footprint(self.h, k))
 
@@ -211,17 +221,21 @@ def poisson_schedule(n_req: int, rate: float, k_lo: int, k_hi: int, seed: int):
     return [(float(t), int(k), 10_000 + i) for i, (t, k) in enumerate(zip(arrivals, ks))]
 
 
-def run_schedule(server: Server, schedule, timeout_s: float = 900.0):
+def run_schedule(server: Server, schedule, timeout_s: float = 900.0, submit=None, wait=None):
     """Submits each (arrival_s, k, seed) at its arrival time, waits for all; returns results
-    and summary statistics (latency = completion - submission, server clock)."""
+    and summary statistics (latency = completion - submission, server clock).  ``submit(k,
+    seed)`` / ``wait(handle)`` replace the built-in program's submission (compiled programs:
+    program.CompiledProgram)."""
+    submit = submit or server.submit
+    wait = wait or (lambda t: server.wait(t, timeout_s))
     start = time.perf_counter()
     tickets = []
     for t_arr, k, seed in schedule:
         delay = t_arr - (time.perf_counter() - start)
         if delay > 0:
             time.sleep(delay)
-        tickets.append(server.submit(k, seed))
-    results = [server.wait(t, timeout_s) for t in tickets]
+        tickets.append(submit(k, seed))
+    results = [wait(t) for t in tickets]
     ok = [r for r in results if r.status == 0]
     lat = np.array([r.done_s - r.submit_s for r in ok]) * 1e3
     span = max(r.done_s for r in ok) - min(r.submit_s for r in ok) if ok else float("nan")
