@@ -635,21 +635,24 @@ def measure_served(zk, bases, args):
     out = {"workload": f"{args.served_requests} requests, Poisson 50 req/s, k uniform 14..22, program = "
                        "3 INTT + coset NTT 4x + fused quotient + 4 MSM (one batch) + 2 evals",
            "hbm_arena_gb": 48}
-    burst = [(0.0, k, seed) for _, k, seed in sched]  # every request at once: capacity
+    burst = [(0.0, k, seed) for _, k, seed in sched[:120]]  # 120 requests at once: capacity
     # resident bases with the tuned (window, tables) per size range
     sets = zk.serving.resident_sets(bases.tables[: bases.n], 14, 22)
     out["table_sets"] = [{"max_k": mk, "window": rb.window, "tables": rb.n_tables} for rb, mk in sets]
-    for name, inflight in (("served", 8), ("served_1_slot", 1)):
+    # the served form's admission policy: at most one request of size >= 2^21 in flight (the
+    # latency tail is made of the largest requests; smaller ones are admitted past a waiting one)
+    policy = {"priority_k": 0, "large_k": 21, "max_large_inflight": 1}
+    out["policy"] = policy
+    for name, inflight, pol in (("served", 8, policy), ("served_no_policy", 8, {}), ("served_1_slot", 1, {})):
         srv = zk.serving.Server(sets, hbm_bytes=48 << 30, max_inflight=inflight, ext_log=2, min_k=14, max_k=22)
+        srv.set_policy(**pol)
         # warm the constants / kernels once
         srv.wait(srv.submit(14, 1))
         _, summary = zk.serving.run_schedule(srv, sched)
         out[name] = summary
-        if inflight > 1:
-            _, cap = zk.serving.run_schedule(srv, burst)
-            out["served_capacity"] = cap
+        _, out[name.replace("served", "served_capacity", 1)] = zk.serving.run_schedule(srv, burst)
         srv.close()
-    out["served_compiled"] = measure_served_compiled(zk, sets, sched, burst)
+    out["served_compiled"] = measure_served_compiled(zk, sets, sched, burst, policy)
     prover = zk.serving.PerCallProver(bases, ext_log=2, max_k=22)
     del sets
     prover.warm(range(14, 23))
@@ -665,7 +668,7 @@ def measure_served(zk, bases, args):
     return out
 
 
-def measure_served_compiled(zk, sets, sched, burst, k_lo=14, k_hi=22, ext=2):
+def measure_served_compiled(zk, sets, sched, burst, policy, k_lo=14, k_hi=22, ext=2):
     """The served workload with every request a compiled program: the prover program of each
     size written in the reference's artifact forms (program.prover_artifact), lowered once and
     registered with an 8-slot server; its MSMs use the same resident table sets.  Unlike the
@@ -677,6 +680,7 @@ def measure_served_compiled(zk, sets, sched, burst, k_lo=14, k_hi=22, ext=2):
     import time
     P = zk.program
     srv = zk.serving.Server(sets, hbm_bytes=48 << 30, max_inflight=8, ext_log=ext, min_k=k_lo, max_k=k_hi)
+    srv.set_policy(**policy)
     progs, inputs = {}, {}
     t0 = time.perf_counter()
     for k in range(k_lo, k_hi + 1):
@@ -906,7 +910,7 @@ def main():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-fused", action="store_true")
     ap.add_argument("--no-served", action="store_true")
-    ap.add_argument("--served-requests", type=int, default=120)
+    ap.add_argument("--served-requests", type=int, default=400)
     ap.add_argument("--ref-msm-log", type=int, default=22)
     ap.add_argument("--ref-ntt-log", type=int, default=24)
     ap.add_argument("--no-cpu", action="store_true")

@@ -166,3 +166,32 @@ def test_per_size_table_sets(zk, bases):
     finally:
         a.close()
         b.close()
+
+
+def test_admission_policy(zk, bases):
+    """With the tail policy (large requests on high-priority streams, at most one of them in
+    flight) every result is still the one the request gets alone, and no two large requests
+    ever run at the same time."""
+    reqs = [(k, 300 + i) for i, k in enumerate([14, 10, 13, 14, 11, 13, 12, 14, 10, 13])]
+    ref = server(zk, bases, 1)
+    try:
+        alone = {seed: zk.serving.result_words(ref.wait(ref.submit(k, seed))) for k, seed in reqs}
+    finally:
+        ref.close()
+    srv = server(zk, bases, 6)
+    try:
+        srv.set_policy(priority_k=13, large_k=13, max_large_inflight=1)
+        tickets = [(k, seed, srv.submit(k, seed)) for k, seed in reqs]
+        res = [(k, seed, srv.wait(t)) for k, seed, t in tickets]
+        assert srv.stats()["peak_inflight"] > 1
+    finally:
+        srv.close()
+    large = []
+    for k, seed, r in res:
+        assert r.status == 0
+        assert np.array_equal(zk.serving.result_words(r), alone[seed]), (k, seed)
+        if k >= 13:
+            large.append((r.start_s, r.done_s))
+    large.sort()
+    for (s0, d0), (s1, d1) in zip(large, large[1:]):
+        assert s1 >= d0  # admitted only after the previous large request completed
