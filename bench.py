@@ -29,9 +29,9 @@ sys.path.insert(0, ROOT)
 
 METRIC = "MSM points/s (2^22) & NTT elems/s (2^24); served p50/p99 vs plain per-call"
 MSM_LOG, NTT_LOG = 22, 24
-# ncu DRAM bytes (read + write) of one whole 2^22 transform (all passes) per element, from the
-# capture summarised in profiles/ntt_passes_ntt2p22.md; traffic grows with the element count
-NTT_TRAFFIC_PER_ELEM = 342.0
+# ncu DRAM bytes (read + write) of one whole 2^24 transform (all five passes) per element, from the
+# capture summarised in profiles/ntt_passes_ntt2p24.md
+NTT_TRAFFIC_PER_ELEM = 398.0
 
 
 def workload_config(world: int) -> dict:
@@ -226,7 +226,154 @@ def run_reference_arm(args):
                          "sample": steps[-1]["msm_sample"] + "; " + steps[-1]["ntt_sample"], "cpu": cpu_model()},
         "e2e": {"value": v, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if not args.no_ref_gpu:
+        line["ref_gpu"] = measure_reference_gpu(steps[-1])
     print(json.dumps(line), flush=True)
+
+
+def measure_reference_gpu(cpu):
+    """The reference's own CUDA kernels for the path, built from its sources for sm_100a
+    (oracle/build_ref.py), timed on this box on the CPU arm's inputs and checked bit for bit
+    against the CPU arm's outputs: ssip_ntt at 2^24 (root table from its ssip_precompute), msm
+    at 2^22 through its host-buffer ABI in the configuration its cost model picks for that size
+    (window 17, 8 target windows: two point tables from its msm_precompute, 16 parts, two
+    stages; host clock, the call is synchronous), and poly_eval / batched_invert / kate_division
+    / scan_mul at 2^22 (CUDA events).  Outside the timed CPU steps; none of this repository's
+    kernels run here."""
+    import ctypes
+    import numpy as np
+    here = os.path.join(ROOT, "oracle", "_ref")
+    names = ("libref_ntt.so", "libref_msm_17_8.so", "libref_poly.so")
+    if not all(os.path.exists(os.path.join(here, n)) for n in names):
+        return {"unavailable": "the reference's kernels were not built (oracle/_ref absent)"}
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return {"unavailable": "no CUDA device"}
+    except ImportError:
+        return {"unavailable": "torch missing"}
+    from oracle import oracle as orc
+
+    class PolyPtr(ctypes.Structure):
+        _fields_ = [("ptr", ctypes.c_void_p), ("len", ctypes.c_size_t), ("rotate", ctypes.c_size_t),
+                    ("offset", ctypes.c_size_t), ("whole_len", ctypes.c_size_t)]
+
+    V, U, UL = ctypes.c_void_p, ctypes.c_uint, ctypes.POINTER(ctypes.c_ulong)
+    ntt = ctypes.CDLL(os.path.join(here, names[0]))
+    ntt.ssip_ntt.argtypes = [PolyPtr, V, U, V, U, U]
+    ntt.ssip_precompute.argtypes = [V, U, V]
+    msm = ctypes.CDLL(os.path.join(here, names[1]))
+    msm.msm.argtypes = [V, V, ctypes.c_ulonglong, U, U, U, U, U, V, V, U, V, V]
+    msm.msm_precompute.argtypes = [ctypes.c_ulonglong, V, U]
+    poly = ctypes.CDLL(os.path.join(here, names[2]))
+    for name, a in (("poly_eval", [V, UL, PolyPtr, V, V, V]), ("batched_invert", [V, UL, PolyPtr, V]),
+                    ("kate_division", [V, UL, U, PolyPtr, V, PolyPtr, V]), ("scan_mul", [V, UL, PolyPtr, V])):
+        getattr(poly, name).argtypes = a
+    for lib in (ntt, msm, poly):
+        for f in ("ssip_ntt", "ssip_precompute", "msm", "msm_precompute", "poly_eval", "batched_invert",
+                  "kate_division", "scan_mul"):
+            if hasattr(lib, f):
+                getattr(lib, f).restype = ctypes.c_int
+    dev = torch.device("cuda", 0)
+    st = torch.cuda.current_stream().cuda_stream
+    out = {"built_from": "the reference's core/src/{ntt,msm,poly}/src sources, nvcc sm_100a (oracle/build_ref.py)"}
+
+    def dev_words(a, words):
+        return torch.from_numpy(np.ascontiguousarray(a).view(np.int32).reshape(-1, words).copy()).to(dev)
+
+    def pp(t, n):
+        return PolyPtr(t.data_ptr(), n, 0, 0, n)
+
+    def events(fn, reps=5):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    # ---- ssip_ntt at the CPU arm's NTT size, on its input
+    L = cpu["logs"][1]
+    n = 1 << L
+    w = np.ascontiguousarray(orc.root_of_unity(L)).view(np.uint32).copy()
+    tw_h = np.zeros((n // 2, 8), dtype=np.uint32)
+    assert ntt.ssip_precompute(tw_h.ctypes.data, n // 2, w.ctypes.data) == 0
+    tw = dev_words(tw_h, 8)
+    x0 = dev_words(cpu["ntt_in"], 8)
+    x = x0.clone()
+    assert ntt.ssip_ntt(pp(x, n), tw.data_ptr(), L, st, 8, 8) == 0
+    torch.cuda.synchronize()
+    got = x.cpu().numpy().view(np.uint64).reshape(-1, 4)
+    ms = events(lambda: ntt.ssip_ntt(pp(x, n), tw.data_ptr(), L, st, 8, 8))
+    out["ssip_ntt"] = {"log_n": L, "ms": ms, "elems_per_s": n / (ms / 1e3),
+                       "matches_cpu_best_fft": bool(np.array_equal(got, cpu["ntt_out"]))}
+    del x, x0, tw
+    # ---- msm at the CPU arm's MSM size, its inputs, through the host-buffer ABI
+    M = cpu["logs"][0]
+    m = 1 << M
+    s_h = np.ascontiguousarray(_CPU_INPUTS[cpu["logs"]][0]).view(np.uint32).reshape(m, 8)
+    p_h = np.ascontiguousarray(_CPU_INPUTS[cpu["logs"]][1]).view(np.uint32).reshape(m, 16)
+    pin = lambda a: torch.from_numpy(a.view(np.int32)).pin_memory().numpy().view(np.uint32)  # noqa: E731
+    s_h, tables = pin(s_h), [pin(p_h), pin(np.zeros_like(p_h))]
+    h_tab = (ctypes.c_void_p * 2)(*[t.ctypes.data for t in tables])
+    assert msm.msm_precompute(m, h_tab, 1) == 0
+    parts = 16 if m >= (1 << 16) else 1
+    cards = (ctypes.c_uint * 1)(0)
+    sizes = (ctypes.c_ulong * 1)()
+    assert msm.msm(None, sizes, m, 1, parts, 2, 2, 1, cards, None, 0, None, None) == 0
+    buf = torch.empty(int(sizes[0]), dtype=torch.uint8, device=dev)
+    bufs = (ctypes.c_void_p * 1)(buf.data_ptr())
+    h_s = (ctypes.c_void_p * 1)(s_h.ctypes.data)
+    res = np.zeros(16, dtype=np.uint32)
+    h_r = (ctypes.c_void_p * 1)(res.ctypes.data)
+    times = []
+    for _ in range(4):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        assert msm.msm(bufs, None, m, 1, parts, 2, 2, 1, cards, h_tab, 1, h_s, h_r) == 0
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t0)
+    best = min(times[1:])
+    out["msm"] = {"log_n": M, "ms": best * 1e3, "points_per_s": m / best, "config": "window 17, 2 tables, 16 parts",
+                  "timing": "host clock, best of 3 after one warm-up (synchronous host-buffer call)",
+                  "matches_cpu_best_multiexp": bool(np.array_equal(res.view(np.uint64), cpu["msm_out"]))}
+    del buf, tables
+    # ---- poly library at 2^22 on seeded inputs (poly_eval checked against Horner)
+    P = 22
+    k = 1 << P
+    p0 = orc.gen_fr(900, k)
+    xh = orc.gen_fr(901, 1)
+    pd, xd = dev_words(p0, 8), dev_words(xh, 8)
+    r = torch.zeros(8, dtype=torch.int32, device=dev)
+    q = torch.zeros((k, 8), dtype=torch.int32, device=dev)
+    inv = pd.clone()
+    scan = pd.clone()
+
+    def temp(fn, *a):
+        size = ctypes.c_ulong(0)
+        assert fn(None, ctypes.byref(size), *a) == 0
+        return torch.empty(max(size.value, 1), dtype=torch.uint8, device=dev), size
+    te, ze = temp(poly.poly_eval, pp(pd, k), None, None, None)
+    ti, zi = temp(poly.batched_invert, pp(inv, k), None)
+    tk, zk_ = temp(poly.kate_division, P, pp(pd, k), None, pp(q, k), None)
+    ts, zs = temp(poly.scan_mul, pp(scan, k), None)
+    assert poly.poly_eval(te.data_ptr(), ctypes.byref(ze), pp(pd, k), r.data_ptr(), xd.data_ptr(), st) == 0
+    torch.cuda.synchronize()
+    eval_ok = bool(np.array_equal(r.cpu().numpy().view(np.uint64), orc.eval_poly(p0, xh[0])))
+    out["poly"] = {"log_n": P, "poly_eval_matches_cpu_horner": eval_ok}
+    for name, fn in (
+            ("poly_eval", lambda: poly.poly_eval(te.data_ptr(), ctypes.byref(ze), pp(pd, k), r.data_ptr(),
+                                                 xd.data_ptr(), st)),
+            ("batched_invert", lambda: poly.batched_invert(ti.data_ptr(), ctypes.byref(zi), pp(inv, k), st)),
+            ("kate_division", lambda: poly.kate_division(tk.data_ptr(), ctypes.byref(zk_), P, pp(pd, k),
+                                                         xd.data_ptr(), pp(q, k), st)),
+            ("scan_mul", lambda: poly.scan_mul(ts.data_ptr(), ctypes.byref(zs), pp(scan, k), st))):
+        out["poly"][name + "_ms"] = events(fn)
+    torch.cuda.synchronize()
+    return out
 
 
 # ------------------------------------------------------------------ GPU arm
@@ -915,6 +1062,8 @@ def main():
     ap.add_argument("--ref-ntt-log", type=int, default=24)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer C-ABI leg (profiling runs)")
+    ap.add_argument("--no-ref-gpu", action="store_true",
+                    help="reference arm: skip timing the reference's own CUDA kernels (oracle/_ref)")
     ap.add_argument("--no-verify", action="store_true",
                     help="skip the bit-exact check of the timed results against the CPU port (profiling runs)")
     ap.add_argument("--ntt-log", type=int, default=24)
