@@ -115,6 +115,11 @@ cudaError_t zkp_msm_device_noalloc(const unsigned int *points_d, unsigned int n_
 /* Bytes of the fixed workspace zkp_msm_device_noalloc uses (compare zkp_msm_workspace_size). */
 unsigned long long zkp_msm_noalloc_capacity(void);
 
+/* CTA size (64, 128 or 256 threads; 0 = 256) of one MSM stage for MSMs planned from now on:
+ * stage 0 the pairing rounds' up pass, 1 their down pass, 2 the XYZZ walk.  Set by the
+ * autotuner (no counterpart in the reference); results do not depend on it. */
+cudaError_t zkp_msm_set_block(unsigned int stage, unsigned int threads);
+
 /* Benchmark support: per-stage CUDA-event timing of the last MSM (see zkp_ntt_profile_enable). */
 void zkp_msm_profile_enable(int on);
 int zkp_msm_profile_read(float *ms, const char **names, int max);

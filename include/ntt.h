@@ -86,6 +86,10 @@ cudaError_t zkp_ntt_roots_device(unsigned int *out_d, unsigned long long count, 
  * the default 12).  Each pass transforms 2^D-element pencils in shared memory, D <= max_digit;
  * a smaller cap means more passes of smaller CTAs.  Plans made after the call use it. */
 cudaError_t zkp_ntt_set_max_digit(unsigned int log_len, unsigned int max_digit);
+/* CTA size (32, 64, 128 or 256 threads; 0 = 128) of the register passes of transforms of
+ * 2^log_len elements (log_len 0: every size), set by the autotuner (no counterpart in the
+ * reference, whose launch shapes follow max_threads_stage*_log).  Results do not depend on it. */
+cudaError_t zkp_ntt_set_block(unsigned int log_len, unsigned int threads);
 
 /* The digit widths, top digit first, of the sub-transform passes the current plan for
  * 2^log_len uses (at most max written); returns the number of passes (0 if log_len is 0 or

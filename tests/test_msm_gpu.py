@@ -266,3 +266,25 @@ def test_msm_narrow_scalars(zk, orc, bits):
         finally:
             zk.msm.set_affine_rounds(-1)
     assert np.array_equal(zk.msm.msm_host(s, p), expect)
+
+
+@pytest.mark.parametrize("threads", [64, 128, 256])
+def test_msm_stage_block_shapes(zk, orc, threads):
+    """The tuner's MSM block shapes (CTA sizes of the pairing rounds and the walk) leave the
+    result unchanged."""
+    lib = zk.native.load("libmsm.so")
+    n = 1 << 15
+    s, p = orc.gen_fr(120, n), orc.gen_points(121, n)
+    zk.msm.set_affine_rounds(3)
+    try:
+        for st in range(3):
+            assert lib.zkp_msm_set_block(st, threads) == 0
+        bases = zk.msm.ResidentBases(p, window=13, n_tables=4)
+        res = torch.zeros(16, dtype=torch.int32, device="cuda")
+        bases.msm(torch.from_numpy(s.view(np.int32).reshape(n, 8).copy()).cuda(), res, bases.workspace())
+        torch.cuda.synchronize()
+        assert np.array_equal(res.cpu().numpy().view(np.uint64), orc.best_multiexp(s, p))
+    finally:
+        zk.msm.set_affine_rounds(-1)
+        zk.tuner.apply_msm_blocks()
+    assert lib.zkp_msm_set_block(3, 128) == 1 and lib.zkp_msm_set_block(0, 96) == 1  # refused

@@ -348,3 +348,20 @@ def test_shoup_entries_reject_misaligned_table(zk):
     lib = zk.native.load("libntt.so")
     assert lib.zkp_ntt_ex_shoup(x.poly_ptr(), tw.values.data_ptr(), sh.data_ptr() + 4, 8, None, None, None) == 1
     assert lib.zkp_ntt_shoup_table(tw.values.data_ptr(), 0, sh.data_ptr(), None) == 1
+
+
+@pytest.mark.parametrize("threads", [32, 64, 128, 256])
+def test_ntt_register_pass_block_shapes(zk, orc, threads):
+    """The tuner's NTT block shape (CTA size of the register passes) leaves results unchanged."""
+    lib = zk.native.load("libntt.so")
+    log_n = 17
+    a = orc.gen_fr(130, 1 << log_n)
+    try:
+        assert lib.zkp_ntt_set_block(log_n, threads) == 0
+        x = to_dev(zk, a)
+        zk.ntt.ntt(x)
+        assert np.array_equal(x.numpy_u64(), orc.ntt(a, log_n))
+    finally:
+        lib.zkp_ntt_set_block(log_n, 0)
+        zk.tuner.apply_ntt_plans()
+    assert lib.zkp_ntt_set_block(log_n, 48) == 1  # refused

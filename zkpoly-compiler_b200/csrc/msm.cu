@@ -133,6 +133,18 @@ inline u32 default_window(u64 n) {
     return best;
 }
 
+// CTA sizes of the stages whose thread count is free (each thread owns its own slots or chunk),
+// set by the tuner through zkp_msm_set_block: pair_up, pair_down, accumulate (0 = 256)
+enum BlockStage { BLK_PAIR_UP = 0, BLK_PAIR_DOWN = 1, BLK_ACCUMULATE = 2, BLK_STAGES = 3 };
+inline std::atomic<u32> *block_settings() {
+    static std::atomic<u32> b[BLK_STAGES];
+    return b;
+}
+inline u32 block_for(BlockStage st) {
+    const u32 v = block_settings()[st].load(std::memory_order_relaxed);
+    return v ? v : 256u;
+}
+
 // Affine pairing rounds (stage 4a below): -1 chooses by size, else a fixed count.
 constexpr u32 MAX_ROUNDS = 4;
 constexpr u32 KA = 64;  // list elements per thread in a pairing round (at most KA / 2 pairs)
@@ -1126,13 +1138,14 @@ cudaError_t run_batch(const Batch &b, const Layout &l, char *ws, cudaStream_t st
         ZK_TRY(scan(cursor, nb + 1, st_next, st_next));
         // Montgomery's trick over the round's pairs
         const u64 T = l.thr[r];
-        const u32 grid = (u32)((T + 255) / 256);
+        const u32 bu = block_for(BLK_PAIR_UP), bd = block_for(BLK_PAIR_DOWN);
+        const u32 grid = (u32)((T + bu - 1) / bu), grid_d = (u32)((T + bd - 1) / bd);
         u32 *prefix = at(l.prefix[r]), *tv = at(l.tvals);
         u32 *out_bkt = at(l.lst_bkt[r % 2]), *out_pts = at(l.lst_pts[r % 2]);
         if (r == 0)
-            pair_up_kernel<true><<<grid, 256, 0, stream>>>(b, walk_bkt, walk_pts, st, nb, T, prefix, tv);
+            pair_up_kernel<true><<<grid, bu, 0, stream>>>(b, walk_bkt, walk_pts, st, nb, T, prefix, tv);
         else
-            pair_up_kernel<false><<<grid, 256, 0, stream>>>(b, walk_bkt, walk_pts, st, nb, T, prefix, tv);
+            pair_up_kernel<false><<<grid, bu, 0, stream>>>(b, walk_bkt, walk_pts, st, nb, T, prefix, tv);
         ZK_TRY(cudaGetLastError());
         prof.mark(kUp[r], stream);
         // batched inverse of the T thread totals (levels as laid out for round 0's count)
@@ -1164,11 +1177,11 @@ cudaError_t run_batch(const Batch &b, const Layout &l, char *ws, cudaStream_t st
         }
         prof.mark(kTree[r], stream);
         if (r == 0)
-            pair_down_kernel<true><<<grid, 256, 0, stream>>>(b, walk_bkt, walk_pts, st, st_next, nb, T, prefix, tv,
-                                                             out_bkt, out_pts);
-        else
-            pair_down_kernel<false><<<grid, 256, 0, stream>>>(b, walk_bkt, walk_pts, st, st_next, nb, T, prefix,
+            pair_down_kernel<true><<<grid_d, bd, 0, stream>>>(b, walk_bkt, walk_pts, st, st_next, nb, T, prefix,
                                                               tv, out_bkt, out_pts);
+        else
+            pair_down_kernel<false><<<grid_d, bd, 0, stream>>>(b, walk_bkt, walk_pts, st, st_next, nb, T, prefix,
+                                                               tv, out_bkt, out_pts);
         ZK_TRY(cudaGetLastError());
         prof.mark(kDown[r], stream);
         walk_bkt = out_bkt;
@@ -1176,13 +1189,13 @@ cudaError_t run_batch(const Batch &b, const Layout &l, char *ws, cudaStream_t st
         live = st_next + nb;
     }
     if (l.chunks) {
+        const u32 ba = block_for(BLK_ACCUMULATE);
+        const u32 ga = (u32)((l.chunks + ba - 1) / ba);
         if (l.rounds)
-            accumulate_kernel<false><<<(u32)((l.chunks + 255) / 256), 256, 0, stream>>>(b, walk_bkt, walk_pts, live,
-                                                                                       bs, pp, pb, pf, chains,
-                                                                                       nchain);
+            accumulate_kernel<false><<<ga, ba, 0, stream>>>(b, walk_bkt, walk_pts, live, bs, pp, pb, pf, chains,
+                                                            nchain);
         else
-            accumulate_kernel<true><<<(u32)((l.chunks + 255) / 256), 256, 0, stream>>>(b, sb, sp, live, bs, pp,
-                                                                                      pb, pf, chains, nchain);
+            accumulate_kernel<true><<<ga, ba, 0, stream>>>(b, sb, sp, live, bs, pp, pb, pf, chains, nchain);
         ZK_TRY(cudaGetLastError());
     }
     prof.mark("accumulate", stream);
@@ -1349,6 +1362,12 @@ extern "C" unsigned int zkp_msm_rounds_for(unsigned long long n, unsigned int wi
 
 // affine pairing rounds for MSMs planned after this call: -1 = by size (the default), else
 // 0..4.  Workspace sizes depend on it, so size queries and runs must see the same setting.
+extern "C" cudaError_t zkp_msm_set_block(unsigned int stage, unsigned int threads) {
+    ZK_CHECK_ARG(stage < msm::BLK_STAGES && (threads == 0 || threads == 64 || threads == 128 || threads == 256));
+    msm::block_settings()[stage].store(threads);
+    return cudaSuccess;
+}
+
 extern "C" cudaError_t zkp_msm_set_affine_rounds(int rounds) {
     ZK_CHECK_ARG(rounds >= -1 && rounds <= (int)msm::MAX_ROUNDS);
     msm::affine_rounds_setting() = rounds;

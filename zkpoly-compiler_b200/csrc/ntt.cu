@@ -355,14 +355,20 @@ __global__ void __launch_bounds__(256) ntt_warp_pass_kernel(PassArgs a) {
 #define ZK_NTT_WARP_PENCILS 1  // pencils per lane group in the register pass (1 or 2)
 #endif
 
+// CTA size of the register passes per transform size, set by the tuner through
+// zkp_ntt_set_block (0 = 128)
+std::atomic<u32> g_warp_block[29];
+
 template <u32 P, bool SH>
 cudaError_t launch_warp_pass(const PassArgs &a, cudaStream_t stream) {
-    // two elements of P pencils per thread; CTAs of 128 threads: at 52 registers (the Shoup
-    // variant) 9 of them fit an SM, 36 warps, against 4 CTAs of 256 (32 warps), 5 % faster.
-    // The kernel keeps __launch_bounds__(256): with a bound of 128 the compiler takes 58
-    // registers and the occupancy gain is gone.
+    // two elements of P pencils per thread; CTAs of 128 threads by default: at 52 registers
+    // (the Shoup variant) 9 of them fit an SM, 36 warps, against 4 CTAs of 256 (32 warps), 5 %
+    // faster.  The kernel keeps __launch_bounds__(256): with a bound of 128 the compiler takes
+    // 58 registers and the occupancy gain is gone.
     const u64 threads = 1ull << (a.L - 1 - (P == 2 ? 1 : 0));
-    const u32 block = (u32)(threads < 128 ? threads : 128);
+    const u32 tuned = a.L < 29 ? g_warp_block[a.L].load(std::memory_order_relaxed) : 0;
+    const u32 want = tuned ? tuned : 128;
+    const u32 block = (u32)(threads < want ? threads : want);
     const u32 grid = (u32)(threads / block);
     switch (a.D) {
         case 1: ntt_warp_pass_kernel<1, P, SH><<<grid, block, 0, stream>>>(a); break;
@@ -1058,6 +1064,17 @@ extern "C" cudaError_t zkp_ntt_set_max_digit(unsigned int log_len, unsigned int 
         for (u32 L = 0; L < 29; L++) ntt::g_max_digit[L].store(max_digit);
     } else {
         ntt::g_max_digit[log_len].store(max_digit);
+    }
+    return cudaSuccess;
+}
+
+extern "C" cudaError_t zkp_ntt_set_block(unsigned int log_len, unsigned int threads) {
+    ZK_CHECK_ARG(log_len <= 28 && (threads == 0 || threads == 32 || threads == 64 || threads == 128 ||
+                                   threads == 256));
+    if (log_len == 0) {
+        for (u32 L = 0; L < 29; L++) ntt::g_warp_block[L].store(threads);
+    } else {
+        ntt::g_warp_block[log_len].store(threads);
     }
     return cudaSuccess;
 }

@@ -20,9 +20,18 @@ from .scalar import require_cuda, stream_handle
 LIB = "libmsm.so"
 
 
+_blocks_applied = False
+
+
 def _lib():
+    global _blocks_applied
     require_cuda()
-    return load(LIB)
+    lib = load(LIB)
+    if not _blocks_applied:
+        _blocks_applied = True
+        from . import tuner
+        tuner.apply_msm_blocks()  # tuned stage CTA sizes for this GPU model, if cached
+    return lib
 
 
 def _u32(a: np.ndarray, words: int) -> np.ndarray:

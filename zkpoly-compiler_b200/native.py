@@ -53,6 +53,7 @@ SIGNATURES = {
         "zkp_ntt_num_passes": (ctypes.c_uint, [ctypes.c_uint]),
         "zkp_ntt_plan_digits": (ctypes.c_uint, [ctypes.c_uint, c_void_p, ctypes.c_uint]),
         "zkp_ntt_set_max_digit": (cudaError_t, [ctypes.c_uint, ctypes.c_uint]),
+        "zkp_ntt_set_block": (cudaError_t, [ctypes.c_uint, ctypes.c_uint]),
         "zkp_ntt_batch_plan_create": (cudaError_t, [c_void_p, ctypes.c_uint, ctypes.POINTER(c_void_p)]),
         "zkp_ntt_batch_run": (cudaError_t, [c_void_p, c_void_p]),
         "zkp_ntt_batch_set_solo_log": (cudaError_t, [ctypes.c_uint]),
@@ -70,6 +71,7 @@ SIGNATURES = {
         "zkp_msm_workspace_size": (ctypes.c_ulonglong, [ctypes.c_ulonglong, ctypes.c_uint, ctypes.c_uint]),
         "zkp_msm_default_window": (ctypes.c_uint, [ctypes.c_ulonglong]),
         "zkp_msm_set_affine_rounds": (cudaError_t, [ctypes.c_int]),
+        "zkp_msm_set_block": (cudaError_t, [ctypes.c_uint, ctypes.c_uint]),
         "zkp_msm_rounds_for": (ctypes.c_uint, [ctypes.c_ulonglong, ctypes.c_uint, ctypes.c_uint]),
         "zkp_msm_device": (cudaError_t, [c_void_p, ctypes.c_ulonglong, c_void_p, ctypes.c_uint, c_void_p,
                                          ctypes.c_ulonglong, ctypes.c_uint, c_void_p, c_void_p]),

@@ -4,8 +4,12 @@ predicts a window from relative cost coefficients instead of measuring).
 
 Tuned parameters:
   - MSM window width c in [8, 20] per log2 n (zkp_msm_device timed on seeded inputs);
+  - MSM (window, precomputed tables) for resident bases per log2 n;
+  - MSM block shapes: the CTA size of the pairing rounds' up and down passes and of the XYZZ
+    walk (zkp_msm_set_block), by coordinate descent at the resident 2^22 configuration;
   - NTT largest digit (sub-transform size 2^D, which sets the pass split and the CTA shape)
-    per log2 n (zkp_ntt_set_max_digit, timed on seeded inputs).
+    per log2 n (zkp_ntt_set_max_digit, timed on seeded inputs);
+  - NTT block shape: the CTA size of the register passes per log2 n (zkp_ntt_set_block).
 The cache is a JSON file next to the libraries.  Below it sit the shipped defaults
 (tuning_defaults.json, winners this tuner measured on B200); without an entry in either the
 libraries' own cost model / default plan is used.
@@ -154,12 +158,89 @@ def tune_ntt(log_ns=range(14, 25), candidates=(8, 9, 10, 11, 12), apply: bool = 
 
 
 def apply_ntt_plans() -> None:
-    """Sets the cached digit caps (if any) for this GPU model in libntt.so."""
+    """Sets the cached digit caps and register-pass CTA sizes (if any) for this GPU model in
+    libntt.so."""
     from . import ntt
-    table = _load().get(_device_key(), {}).get("ntt_max_digit", {})
+    dev = _load().get(_device_key(), {})
     lib = load(ntt.LIB)
-    for L, d in table.items():
+    for L, d in dev.get("ntt_max_digit", {}).items():
         check(lib.zkp_ntt_set_max_digit(int(L), int(d)), "zkp_ntt_set_max_digit")
+    for L, t in dev.get("ntt_block", {}).items():
+        check(lib.zkp_ntt_set_block(int(L), int(t)), "zkp_ntt_set_block")
+
+
+MSM_BLOCK_STAGES = ("pair_up", "pair_down", "accumulate")  # zkp_msm_set_block stage ids 0, 1, 2
+
+
+def apply_msm_blocks() -> None:
+    """Sets the cached MSM stage CTA sizes (if any) for this GPU model in libmsm.so."""
+    from . import msm
+    table = _load().get(_device_key(), {}).get("msm_block", {})
+    lib = load(msm.LIB)
+    for i, name in enumerate(MSM_BLOCK_STAGES):
+        if name in table:
+            check(lib.zkp_msm_set_block(i, int(table[name])), "zkp_msm_set_block")
+
+
+def tune_ntt_blocks(log_ns=range(18, 25), candidates=(64, 128, 256)) -> dict:
+    """Times the library's forward NTT of 2^L seeded elements (its tuned digit plan) for each
+    register-pass CTA size and caches the fastest per size."""
+    from . import gen, ntt
+    from .scalar import ScalarArray
+    lib = load(ntt.LIB)
+    apply_ntt_plans()
+    out, times = {}, {}
+    for L in log_ns:
+        x = ScalarArray(gen.fr(81, 1 << L))
+        best = None
+        for t in candidates:
+            check(lib.zkp_ntt_set_block(L, t), "zkp_ntt_set_block")
+            ms = _time(lambda: ntt.ntt(x), reps=10 if L < 22 else 4)
+            times[f"{L}:{t}"] = ms
+            if best is None or ms < best[1]:
+                best = (t, ms)
+        out[str(L)] = best[0]
+        check(lib.zkp_ntt_set_block(L, best[0]), "zkp_ntt_set_block")
+        del x
+    with _lock:
+        _load().setdefault(_device_key(), {})["ntt_block"] = out
+        _save()
+    return {"best": out, "ms": times}
+
+
+def tune_msm_blocks(log_n: int = 22, candidates=(64, 128, 256), bases=None, sweeps: int = 1) -> dict:
+    """Coordinate descent over the CTA sizes of the pairing rounds' up pass, down pass and the
+    XYZZ walk, timing an MSM over resident bases in the tuned (window, tables) configuration
+    of 2^log_n points; caches the winners."""
+    from . import gen, msm
+    n = 1 << log_n
+    lib = load(msm.LIB)
+    pts = bases if bases is not None else gen.points(2, n)
+    c, nt = msm_resident_config(n)
+    rb = msm.ResidentBases(pts, window=c, n_tables=nt)
+    ws = rb.workspace()
+    s = gen.fr(82, n)
+    res = torch.zeros(16, dtype=torch.int32, device="cuda")
+    cur = {name: 256 for name in MSM_BLOCK_STAGES}
+    cur.update(_load().get(_device_key(), {}).get("msm_block", {}))
+    times = {}
+    for _ in range(sweeps):
+        for i, name in enumerate(MSM_BLOCK_STAGES):
+            best = None
+            for t in candidates:
+                check(lib.zkp_msm_set_block(i, t), "zkp_msm_set_block")
+                ms = _time(lambda: rb.msm(s, res, ws), reps=3)
+                times[f"{name}:{t}"] = ms
+                if best is None or ms < best[1]:
+                    best = (t, ms)
+            cur[name] = best[0]
+            check(lib.zkp_msm_set_block(i, best[0]), "zkp_msm_set_block")
+    with _lock:
+        _load().setdefault(_device_key(), {})["msm_block"] = dict(cur)
+        _save()
+    del rb, ws
+    torch.cuda.empty_cache()
+    return {"best": cur, "ms": times}
 
 
 def tune_msm_resident(log_n: int = 22, windows=(13, 14, 15, 16, 17, 18, 19, 20), full_only: bool = True,
