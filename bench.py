@@ -486,6 +486,10 @@ def run_gpu(args):
     native.profile_enable("libmsm.so", False)
     stage_ms = {k: statistics.median(v) for k, v in stages.items()}
 
+    # ---- plain Pippenger over one table (no precomputation): the 2^22 bench size and the 2^20
+    # size of the plain-MSM configuration, device-resident inputs, CUDA events
+    one_table = measure_one_table_msm(zk, scalars, points, stream) if rank == 0 else None
+
     # ---- IMAD peak probe (measured on this GPU)
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
     probe_out = torch.empty(sms * 8 * 256, dtype=torch.int32, device=dev)
@@ -554,7 +558,40 @@ def run_gpu(args):
         verified = verify_outputs(cpu, timed_out, e2e_out if rank == 0 else None)
     emit(args, zk, rank, world, n_msm, n_ntt, ntt_ms, msm_ms, step_ms, pass_ms, bitrev_ms, stage_ms, imad_per_s,
          e2e_msm_s, e2e_ntt_s, cpu, clocks, bases, batched, served, fused, mont_per_s, poly, pipelined,
-         ssip_ms, shoup_per_s, verified)
+         ssip_ms, shoup_per_s, verified, one_table)
+
+
+def measure_one_table_msm(zk, scalars, points, stream, reps=3):
+    """zkp_msm_device over the plain bases (one table, the tuned one-table window, the library's
+    pairing rounds) at the bench's MSM size and at 2^20, on prefixes of the same inputs."""
+    import torch
+    lib = zk.native.load("libmsm.so")
+    out = {}
+    for log_n in sorted({MSM_LOG, 20}):
+        n = 1 << log_n
+        if n > points.shape[0]:
+            continue
+        w = zk.tuner.msm_window(n)
+        ws = torch.empty(zk.msm.workspace_size(n, w), dtype=torch.uint8, device=points.device)
+        res = torch.zeros(16, dtype=torch.int32, device=points.device)
+
+        def run():
+            zk.native.check(lib.zkp_msm_device(ws.data_ptr(), ws.numel(), points.data_ptr(), 1, scalars.data_ptr(),
+                                               n, w, res.data_ptr(), stream.cuda_stream), "zkp_msm_device")
+        run()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            run()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        out[f"2^{log_n}"] = {"ms": ms, "points_per_s": n / (ms / 1e3), "window": w or zk.msm.default_window(n),
+                             "pairing_rounds": zk.msm.rounds_for(n, w, 1)}
+        del ws
+    torch.cuda.empty_cache()
+    return out
 
 
 def measure_fused(zk, gen, dev, stream, hbm_peak, mont_peak, shoup_peak, log_n=NTT_LOG, ext=3, reps=10):
@@ -916,7 +953,7 @@ def run_e2e(zk, native, lib_msm, scalars, points, ntt_in, tw, stream, dev, local
 
 def emit(args, zk, rank, world, n_msm, n_ntt, ntt_ms, msm_ms, step_ms, pass_ms, bitrev_ms, stage_ms, imad_per_s,
          e2e_msm_s, e2e_ntt_s, cpu, clocks, bases, batched=None, served=None, fused=None, mont_per_s=None,
-         poly=None, pipelined=None, ssip_ms=None, shoup_per_s=None, verified=None):
+         poly=None, pipelined=None, ssip_ms=None, shoup_per_s=None, verified=None, one_table=None):
     import torch
     if rank != 0:
         if world > 1:
@@ -1033,6 +1070,10 @@ def emit(args, zk, rank, world, n_msm, n_ntt, ntt_ms, msm_ms, step_ms, pass_ms, 
         line["batched"] = batched
     if served:
         line["served"] = served
+    if one_table:
+        line["msm"]["one_table"] = one_table
+        line["msm"]["one_table_note"] = ("plain Pippenger without precomputed tables (zkp_msm_device, device-resident "
+                                         "inputs), outside the timed region")
     if verified is not None:
         line["verified"], line["verification"] = verified
     if cpu:
