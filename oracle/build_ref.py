@@ -18,14 +18,16 @@ The GPU libraries serve the parity tests that run the reference's kernels next t
 repository's on the same inputs.
 
 Usage: python oracle/build_ref.py [reference_root]
-The checkout is the argument, else $ZKPOLY_REFERENCE_DIR; with neither, nothing is built.
+The checkout is the argument, else $ZKPOLY_REFERENCE_DIR, else a directory named `reference`
+beside this repository's own directory; when none exists, nothing is built.
 """
 import os
 import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("ZKPOLY_REFERENCE_DIR", "")
+REF = (sys.argv[1] if len(sys.argv) > 1 else os.environ.get("ZKPOLY_REFERENCE_DIR")
+       or os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference"))
 OUT_DIR = os.path.join(HERE, "_ref")
 NVCC = "/usr/local/cuda/bin/nvcc"
 BASE = [NVCC, "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared", "-gencode", "arch=compute_100a,code=sm_100a",
