@@ -119,3 +119,19 @@ def test_malformed_program_refused(zk, server):
     t = server.lib.zkp_serve_submit_program(server.h, h, None, 0, None, 0)
     assert server.wait(t).status == 0
     server.lib.zkp_serve_program_destroy(server.h, h)
+
+
+def test_program_destroyed_with_requests_in_flight(zk, orc, server):
+    """Destroying a program whose requests are still queued or running defers the release to
+    the last of them: each still completes with its results, and the program takes no more."""
+    prog = zk.program.CompiledProgram.load(server, ART, zk.program.prover_input_types(10),
+                                           fused=zk.program.prover_fused_graphs())
+    seeds = (31, 32, 33)
+    tickets = [(seed, prog.submit(_inputs(orc, 10, seed))) for seed in seeds]
+    server.lib.zkp_serve_program_destroy(server.h, prog.h)
+    handle, prog.h = prog.h, None
+    for seed, t in tickets:
+        r, leaves = prog.wait(t)
+        assert r.status == 0
+        assert np.array_equal(_words(leaves), expected(orc, 10, seed)), seed
+    del handle

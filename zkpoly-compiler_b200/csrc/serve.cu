@@ -137,7 +137,8 @@ struct ZkpProgram {
     u64 device_bytes = 0, host_bytes = 0, result_extent = 0;
     std::vector<ZkpProgOut> outs;
     std::vector<u64> input_bytes;
-    std::atomic<long long> live{0};  // requests submitted and not yet completed
+    long long live = 0;     // requests submitted and not yet completed (under the server mutex)
+    bool orphaned = false;  // destroyed while requests were live: freed by the last one
 };
 
 struct ZkpServer {
@@ -486,7 +487,11 @@ cudaError_t launch_compiled(ZkpServer *s, Request *r, ZkpServer::Slot &slot) {
 }
 
 void finish(ZkpServer *s, Request *r, int status) {
-    if (r->prog) const_cast<ZkpProgram *>(r->prog)->live--;
+    if (r->prog) {  // called with the server mutex held
+        auto *p = const_cast<ZkpProgram *>(r->prog);
+        if (--p->live == 0 && p->orphaned) delete p;
+        r->prog = nullptr;
+    }
     r->res.status = status;
     r->res.done_s = s->now();
     r->done = true;
@@ -870,14 +875,13 @@ extern "C" long long zkp_serve_submit_program(ZkpServer *s, const ZkpProgram *pr
     auto *r = new Request();
     memset(&r->req, 0, sizeof(r->req));
     memset(&r->res, 0, sizeof(r->res));
-    r->prog = prog;
-    const_cast<ZkpProgram *>(prog)->live++;
     std::lock_guard<std::mutex> g(s->mu);
-    if (s->stop) {
-        const_cast<ZkpProgram *>(prog)->live--;
+    if (s->stop || prog->orphaned) {
         delete r;
         return -1;
     }
+    r->prog = prog;
+    const_cast<ZkpProgram *>(prog)->live++;
     r->ticket = s->next_ticket++;
     r->res.submit_s = s->now();
     s->all[r->ticket] = r;
@@ -904,6 +908,10 @@ extern "C" long long zkp_serve_submit_program(ZkpServer *s, const ZkpProgram *pr
 }
 
 extern "C" void zkp_serve_program_destroy(ZkpServer *s, ZkpProgram *prog) {
-    (void)s;
-    delete prog;
+    if (!s || !prog) return;
+    std::lock_guard<std::mutex> g(s->mu);
+    if (prog->live > 0)
+        prog->orphaned = true;  // the last of its requests to finish frees it
+    else
+        delete prog;
 }

@@ -734,7 +734,11 @@ class CompiledProgram:
         return r, out
 
     def close(self):
+        """Waits for this program's outstanding requests (their input and result buffers live
+        in this object), then destroys the native program."""
         if self.h:
+            for t in list(self._live):
+                self.wait(t)
             self.server.lib.zkp_serve_program_destroy(self.server.h, self.h)
             self.h = None
 
