@@ -192,7 +192,8 @@ cudaError_t zkp_serve_program_create(ZkpServer *s, const ZkpProgOp *ops, unsigne
  * request's ZkpProverResult carries status, times and footprint; msm / evals are unused. */
 long long zkp_serve_submit_program(ZkpServer *s, const ZkpProgram *prog, const void *const *inputs,
                                    unsigned int n_inputs, void *results, unsigned long long results_bytes);
-/* Destroys a program; no request of it may be pending or running. */
+/* Destroys a program.  Its requests still pending or running complete normally and the last
+ * of them releases it; no request may be submitted to it afterwards. */
 void zkp_serve_program_destroy(ZkpServer *s, ZkpProgram *prog);
 
 #ifdef __cplusplus

@@ -123,7 +123,7 @@ def test_malformed_program_refused(zk, server):
 
 def test_program_destroyed_with_requests_in_flight(zk, orc, server):
     """Destroying a program whose requests are still queued or running defers the release to
-    the last of them: each still completes with its results, and the program takes no more."""
+    the last of them: each still completes with its results."""
     prog = zk.program.CompiledProgram.load(server, ART, zk.program.prover_input_types(10),
                                            fused=zk.program.prover_fused_graphs())
     seeds = (31, 32, 33)
