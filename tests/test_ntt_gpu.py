@@ -365,3 +365,34 @@ def test_ntt_register_pass_block_shapes(zk, orc, threads):
         lib.zkp_ntt_set_block(log_n, 0)
         zk.tuner.apply_ntt_plans()
     assert lib.zkp_ntt_set_block(log_n, 48) == 1  # refused
+
+
+@pytest.mark.parametrize("log_in,log_out", [(18, 20), (20, 21)])
+def test_coset_elementwise_prep_sizes(zk, orc, log_in, log_out):
+    """From 2^20 the coset shift and the zero-extension run as one elementwise pass before the
+    transform.  Montgomery and Shoup twiddles, rotated source and destination views, and the
+    in-place shift + scale form, each against the oracle."""
+    n_in, n_out = 1 << log_in, 1 << log_out
+    coef = orc.gen_fr(150 + log_in, n_in)
+    seven = orc.to_mont(orc.int_to_limbs(7))
+    tw = zk.ntt.twiddle_table(log_out)
+    sh = zk.ntt.shoup_table_of(tw)
+    expect = orc.coset_ntt(coef, log_in, log_out, seven)
+    out = zk.ScalarArray.zeros(n_out)
+    zk.ntt.coset_lde(out, to_dev(zk, coef), tw, zk.ntt.scalar_const(7))
+    assert np.array_equal(out.numpy_u64(), expect)
+    # rotated source (element i of the view is coef[(i - 5) mod n_in]) into a rotated destination
+    src = zk.ScalarArray(to_dev(zk, coef).values, length=n_in, rotate=5)
+    dst_base = zk.ScalarArray.zeros(n_out)
+    dst = zk.ScalarArray(dst_base.values, length=n_out, rotate=9)
+    zk.ntt.coset_lde(dst, src, tw, zk.ntt.scalar_const(7), shoup=sh)
+    logical = orc.poly_ptr_view(coef, n_in, rotate=5)
+    expect_rot = orc.coset_ntt(logical, log_in, log_out, seven)
+    assert np.array_equal(orc.poly_ptr_view(dst_base.numpy_u64(), n_out, rotate=9), expect_rot)
+    # in place: x <- 3 * NTT(5^i x_i) at the output size
+    a = orc.gen_fr(160 + log_out, n_out)
+    x = to_dev(zk, a)
+    zk.ntt.ntt_ex(x, tw, shift=zk.ntt.scalar_const(5), scale=zk.ntt.scalar_const(3), shoup=sh)
+    three = orc.to_mont(orc.int_to_limbs(3))
+    want = orc.coset_ntt(a, log_out, log_out, orc.to_mont(orc.int_to_limbs(5)))
+    assert np.array_equal(x.numpy_u64(), orc.vec_mul(want, np.tile(three, (n_out, 1))))

@@ -243,22 +243,25 @@ def tune_msm_blocks(log_n: int = 22, candidates=(64, 128, 256), bases=None, swee
     return {"best": cur, "ms": times}
 
 
-def tune_msm_resident(log_n: int = 22, windows=(13, 14, 15, 16, 17, 18, 19, 20), full_only: bool = True,
-                      bases=None) -> tuple:
-    """Times zkp_msm_device over precomputed tables (one per window when full_only) for each
-    window width and caches the fastest (window, n_tables) for resident bases of 2^log_n."""
+def tune_msm_resident(log_n: int = 22, windows=range(8, 21), full_only: bool = True, bases=None,
+                      batch: int = 4) -> tuple:
+    """Times `batch` MSMs of 2^log_n points in one zkp_msm_batch launch sequence over
+    precomputed tables (one per window when full_only) for each window width and caches the
+    fastest (window, n_tables) for resident bases of 2^log_n.  The default batch of 4 is the
+    served program's shape (its four MSMs run as one batch); batch=1 tunes for single calls."""
     from . import gen, msm
     n = 1 << log_n
     pts = bases if bases is not None else gen.points(2, n)
-    s = gen.fr(78, n)
-    res = torch.zeros(16, dtype=torch.int32, device="cuda")
+    scalars = [gen.fr(78 + i, n) for i in range(batch)]
+    res = [torch.zeros(16, dtype=torch.int32, device="cuda") for _ in range(batch)]
     results = {}
     for c in windows:
         nt = (254 + c - 1) // c if full_only else 1
-        rb = msm.ResidentBases(pts, window=c, n_tables=nt)
-        ws = rb.workspace()
-        results[(c, nt)] = _time(lambda: rb.msm(s, res, ws), reps=2)
-        del rb, ws
+        rb = msm.ResidentBases(pts[:n], window=c, n_tables=nt)
+        b = msm.MsmBatch([{"points": rb.tables, "n_tables": rb.n_tables, "table_stride": rb.n, "scalars": s,
+                           "n": n, "window": c, "result": r} for s, r in zip(scalars, res)])
+        results[(c, nt)] = _time(lambda: b.run(), reps=3)
+        del rb, b
         torch.cuda.empty_cache()
     best = min(results, key=results.get)
     with _lock:
