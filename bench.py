@@ -527,7 +527,7 @@ def run_gpu(args):
     torch.cuda.synchronize()
     shoup_per_s = 5 * sms * 8 * 256 * mont_iters * 2 / (e0.elapsed_time(e1) / 1e3)
 
-    # ---- fused quotient kernel on the 2^24 extended coset (north_star's fused-kernel roofline)
+    # ---- fused quotient kernel on the 2^24 extended coset (its HBM and product rooflines)
     fused = measure_fused(zk, gen, dev, stream, hbm_peak=peaks()[0],
                           mont_peak=mont_per_s, shoup_peak=shoup_per_s) if not args.no_fused else None
 
@@ -1014,7 +1014,7 @@ def emit(args, zk, rank, world, n_msm, n_ntt, ntt_ms, msm_ms, step_ms, pass_ms, 
                         "table of 64 B per root, both built once outside the timed region)",
                 "ssip_ms": ssip_ms, "ssip_value": world * n_ntt / (ssip_ms / 1e3) if ssip_ms else None,
                 "ssip_path": "ssip_ntt (reference ABI): the same passes with Montgomery twiddle products"},
-        # the NTT's roofline by north_star's accounting: 64 B per element (one read + one write
+        # the NTT's HBM roofline: 64 B per element (one read + one write
         # of the vector) for the whole transform, over the transform's CUDA-event time
         "roofline": {"kernel": f"NTT 2^{NTT_LOG} forward transform: {len(digits)} register passes "
                                f"(ntt_warp_pass_kernel, the last fused with the bit reversal in "
