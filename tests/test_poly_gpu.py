@@ -130,6 +130,19 @@ def test_scalar_inv_and_pow(zk, orc):
     assert not z.cpu().numpy().any()
 
 
+def test_scalar_inv_edge_words(zk, orc):
+    """The inversion (batched binary-GCD steps, fixed 17 x 30 iterations) on the stored words
+    it inverts: small values, values next to m and to powers of two, R mod m, R^2 mod m, and
+    seeded values; each equals the oracle's Montgomery inverse."""
+    words = [1, 2, 3, 5, M - 1, M - 2, (M - 1) // 2, (M + 1) // 2, 1 << 253, (1 << 254) % M, (1 << 128) + 1,
+             (1 << 32) - 1, R % M, R * R % M, M - (1 << 200)]
+    vals = [orc.int_to_limbs(w) for w in words] + list(orc.gen_fr(13, 48))
+    for x in vals:
+        t = scal(zk, x)
+        zk.poly.inv_scalar(t)
+        assert np.array_equal(t.cpu().numpy().view(np.uint64)[0], orc.inv(x)), orc.limbs_to_int(x)
+
+
 def test_square_matches_mul(zk, orc):
     """The dedicated Montgomery squaring equals a * a bit for bit (edge values included)."""
     n = 20000

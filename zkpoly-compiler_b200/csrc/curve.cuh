@@ -254,89 +254,183 @@ ZK_DI G1X g1_mul_u64(const G1X &p, u64 k) {
     return acc;
 }
 
-// ------------------------------------------------------------------ inversion for the
-// latency-critical single-thread tail: binary extended Euclid on plain integers.
-// Input a = x R mod q (Montgomery form, x != 0); returns x^-1 R mod q.
-ZK_DI void bn_rshift1(u32 *a) {
+// ------------------------------------------------------------------ inversion
+// Binary extended GCD with batched steps (T. Pornin, "Optimized Binary GCD for Modular
+// Inversion", IACR ePrint 2020/972, algorithm 2 with k - 1 = 30).  With a = y, b = m, u = 1,
+// v = 0 and t steps taken, a 2^t = y u and b 2^t = y v (mod m).  A step halves a when it is
+// even; otherwise it swaps (a, b), (u, v) when a < b and replaces a by (a - b) / 2, u by u - v;
+// every step doubles v.  Each of 17 outer iterations takes 30 steps on 62-bit approximations of
+// a and b (their low 30 bits below their top 32 bits, at a common bit length n >= 62), collects
+// them in signed factors f0, g0, f1, g1 (|f| + |g| <= 2^30 per row), then applies them to the
+// full values: a <- (a f0 + b g0) / 2^30, b <- (a f1 + b g1) / 2^30 (exact; a negative result is
+// negated with its row), and u, v by one Montgomery step each, (u f + v g) 2^-32 mod m.  After
+// 510 steps a = 0 and b = gcd = 1, so y^-1 = v 2^(32 * 17 - 510) = v 2^34.  The iteration counts
+// are fixed and every step is a select, so the threads of a warp never diverge.
+ZK_DI void mul_small9(const u32 *x, u32 c, u32 *r) {
+    u64 carry = 0;
 #pragma unroll
-    for (int i = 0; i < 7; i++) a[i] = (a[i] >> 1) | (a[i + 1] << 31);
-    a[7] >>= 1;
-}
-ZK_DI bool bn_is_one(const u32 *a) {
-    u32 acc = a[0] ^ 1u;
-#pragma unroll
-    for (int i = 1; i < 8; i++) acc |= a[i];
-    return acc == 0;
-}
-ZK_DI bool bn_geq(const u32 *a, const u32 *b) {
-    for (int i = 7; i >= 0; i--) {
-        if (a[i] != b[i]) return a[i] > b[i];
+    for (int i = 0; i < 8; i++) {
+        const u64 t = (u64)x[i] * c + carry;
+        r[i] = (u32)t;
+        carry = t >> 32;
     }
-    return true;
+    r[8] = (u32)carry;
 }
-// (x + q) / 2 or x / 2 modulo q for x < q
+ZK_DI void neg9_if(u32 *r, bool neg) {
+    const u32 mask = neg ? 0xffffffffu : 0u;
+    u64 c = neg ? 1u : 0u;
+#pragma unroll
+    for (int i = 0; i < 9; i++) {
+        const u64 t = (u64)(r[i] ^ mask) + c;
+        r[i] = (u32)t;
+        c = t >> 32;
+    }
+}
+// |x f + y g| / 2^30 into out (x, y < 2^255, |f| + |g| <= 2^30, the sum divisible by 2^30);
+// returns whether x f + y g is negative
+ZK_DI bool lin_shift30(const u32 *x, int f, const u32 *y, int g, u32 *out) {
+    u32 p[9], q[9], s[9];
+    mul_small9(x, (u32)(f < 0 ? -f : f), p);
+    neg9_if(p, f < 0);
+    mul_small9(y, (u32)(g < 0 ? -g : g), q);
+    neg9_if(q, g < 0);
+    u64 c = 0;
+#pragma unroll
+    for (int i = 0; i < 9; i++) {
+        const u64 t = (u64)p[i] + q[i] + c;
+        s[i] = (u32)t;
+        c = t >> 32;
+    }
+    const bool neg = (s[8] >> 31) != 0;
+    neg9_if(s, neg);
+#pragma unroll
+    for (int i = 0; i < 8; i++) out[i] = (s[i] >> 30) | (s[i + 1] << 2);
+    return neg;
+}
+// (u f + v g) 2^-32 mod m into out, for u, v < m and |f| + |g| <= 2^30
 template <class P>
-ZK_DI void half_mod(u32 *x) {
-    if (x[0] & 1u) {
-        u32 c;
-        x[0] = add_cc(x[0], P::m(0));
+ZK_DI void coef_step(const u32 *u, int f, const u32 *v, int g, u32 *out) {
+    u32 uu[8], vv[8], p[9], q[9], x[9];
+    // a negative factor multiplies m - u instead (m when u = 0, still within the bound)
+    {
+        u32 bu = 0, bv = 0;
+        const u32 mu = f < 0 ? 0xffffffffu : 0u, mv = g < 0 ? 0xffffffffu : 0u;
 #pragma unroll
-        for (int i = 1; i < 8; i++) x[i] = addc_cc(x[i], P::m(i));
-        c = addc(0u, 0u);
-        bn_rshift1(x);
-        x[7] |= c << 31;
-    } else {
-        bn_rshift1(x);
+        for (int i = 0; i < 8; i++) {
+            const u64 tu = (u64)P::m(i) - u[i] - bu;
+            const u64 tv = (u64)P::m(i) - v[i] - bv;
+            bu = (u32)(tu >> 32) & 1u;
+            bv = (u32)(tv >> 32) & 1u;
+            uu[i] = ((u32)tu & mu) | (u[i] & ~mu);
+            vv[i] = ((u32)tv & mv) | (v[i] & ~mv);
+        }
     }
+    mul_small9(uu, (u32)(f < 0 ? -f : f), p);
+    mul_small9(vv, (u32)(g < 0 ? -g : g), q);
+    u64 c = 0;
+#pragma unroll
+    for (int i = 0; i < 9; i++) {
+        const u64 t = (u64)p[i] + q[i] + c;
+        x[i] = (u32)t;
+        c = t >> 32;
+    }
+    // x < m 2^30; (x + k m) / 2^32 < 2m with k = x * (-m^-1) mod 2^32
+    const u32 k = x[0] * P::MPRIME;
+    c = ((u64)P::m(0) * k + x[0]) >> 32;
+#pragma unroll
+    for (int i = 1; i < 8; i++) {
+        const u64 t = (u64)P::m(i) * k + x[i] + c;
+        out[i - 1] = (u32)t;
+        c = t >> 32;
+    }
+    out[7] = (u32)((u64)x[8] + c);
+    // conditional subtraction of m
+    u32 d[8], br = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        const u64 t = (u64)out[i] - P::m(i) - br;
+        d[i] = (u32)t;
+        br = (u32)(t >> 32) & 1u;
+    }
+#pragma unroll
+    for (int i = 0; i < 8; i++) out[i] = br ? out[i] : d[i];
+}
+// bits [s, s + 32) of the 256-bit x (s < 256), with x's limbs picked by selects, not indexing
+ZK_DI u32 bits32_at(const u32 *x, u32 s) {
+    const u32 w = s >> 5, sh = s & 31;
+    u32 lo = 0, hi = 0;
+#pragma unroll
+    for (u32 i = 0; i < 8; i++) {
+        lo = i == w ? x[i] : lo;
+        hi = i == w + 1 ? x[i] : hi;
+    }
+    return __funnelshift_r(lo, hi, sh);
 }
 
+// Input a = x R mod m (Montgomery form, x != 0); returns x^-1 R mod m (0 for 0).
 template <class P>
 ZK_DI Fp<P> inv_binary(const Fp<P> &a_mont) {
     using F = Fp<P>;
-    F a = a_mont.canonical();
-    if (a.is_zero()) return F::zero();
-    u32 u[8], v[8], x1[8], x2[8];
+    const F y = a_mont.canonical();
+    if (y.is_zero()) return F::zero();
+    u32 a[8], b[8], u[8], v[8];
 #pragma unroll
     for (int i = 0; i < 8; i++) {
-        u[i] = a.v[i];
-        v[i] = P::m(i);
-        x1[i] = 0;
-        x2[i] = 0;
+        a[i] = y.v[i];
+        b[i] = P::m(i);
+        u[i] = 0;
+        v[i] = 0;
     }
-    x1[0] = 1;
-    // invariant: x1 * a == u, x2 * a == v (mod q)
-    while (!bn_is_one(u) && !bn_is_one(v)) {
-        while ((u[0] & 1u) == 0) {
-            bn_rshift1(u);
-            half_mod<P>(x1);
-        }
-        while ((v[0] & 1u) == 0) {
-            bn_rshift1(v);
-            half_mod<P>(x2);
-        }
-        if (bn_geq(u, v)) {
-            F::sub_raw(u, u, v);
-            F t1 = F::from_words(x1), t2 = F::from_words(x2);
-            F d = F::sub_c(t1, t2);
+    u[0] = 1;
+    for (int it = 0; it < 17; it++) {
+        // common length n = max(len a, len b, 62)
+        u32 n = 62;
 #pragma unroll
-            for (int i = 0; i < 8; i++) x1[i] = d.v[i];
-        } else {
-            F::sub_raw(v, v, u);
-            F t1 = F::from_words(x1), t2 = F::from_words(x2);
-            F d = F::sub_c(t2, t1);
+        for (u32 i = 0; i < 8; i++) {
+            const u32 o = a[i] | b[i];
+            const u32 len = o ? 32 * i + 32 - __clz(o) : 0u;
+            n = len > n ? len : n;
+        }
+        u64 ab = ((u64)bits32_at(a, n - 32) << 30) | (a[0] & 0x3fffffffu);
+        u64 bb = ((u64)bits32_at(b, n - 32) << 30) | (b[0] & 0x3fffffffu);
+        int f0 = 1, g0 = 0, f1 = 0, g1 = 1;
+#pragma unroll 10
+        for (int j = 0; j < 30; j++) {
+            const bool odd = (ab & 1u) != 0;
+            const bool sw = odd && ab < bb;
+            const u64 ta = sw ? bb : ab, tb = sw ? ab : bb;
+            const int tf0 = sw ? f1 : f0, tg0 = sw ? g1 : g0, tf1 = sw ? f0 : f1, tg1 = sw ? g0 : g1;
+            ab = (odd ? ta - tb : ta) >> 1;
+            bb = tb;
+            f0 = odd ? tf0 - tf1 : tf0;
+            g0 = odd ? tg0 - tg1 : tg0;
+            f1 = tf1 * 2;
+            g1 = tg1 * 2;
+        }
+        u32 na[8], nb[8], nu[8], nv[8];
+        if (lin_shift30(a, f0, b, g0, na)) {
+            f0 = -f0;
+            g0 = -g0;
+        }
+        if (lin_shift30(a, f1, b, g1, nb)) {
+            f1 = -f1;
+            g1 = -g1;
+        }
+        coef_step<P>(u, f0, v, g0, nu);
+        coef_step<P>(u, f1, v, g1, nv);
 #pragma unroll
-            for (int i = 0; i < 8; i++) x2[i] = d.v[i];
+        for (int i = 0; i < 8; i++) {
+            a[i] = na[i];
+            b[i] = nb[i];
+            u[i] = nu[i];
+            v[i] = nv[i];
         }
     }
-    F r = bn_is_one(u) ? F::from_words(x1) : F::from_words(x2);
-    // r = (xR)^-1 = x^-1 R^-1.  Each Montgomery product with R^2 multiplies by R:
-    // x^-1 R^-1 -> x^-1 -> x^-1 R (the Montgomery form of x^-1)
-    F r2;
+    // v = y^-1 2^-34, and x^-1 R = y^-1 R^2 = Montgomery product of v and 2^34 R^3
+    F k;
 #pragma unroll
-    for (int i = 0; i < 8; i++) r2.v[i] = P::r2(i);
-    r = F::mul(r, r2);
-    r = F::mul(r, r2);
-    return r.canonical();
+    for (int i = 0; i < 8; i++) k.v[i] = P::invk(i);
+    return F::mul(F::from_words(v), k).canonical();
 }
 
 // XYZZ -> affine (scaling-z, curve_xyzz.cuh:316-322); identity -> (0, 0)

@@ -59,6 +59,12 @@ struct FrParams {
         return t[i];
     }
     static constexpr u32 MPRIME = 4026531839u;  // -m^-1 mod 2^32
+    // 2^34 R^3 mod m: the final factor of inv_binary (curve.cuh)
+    ZK_DI static constexpr u32 invk(int i) {
+        constexpr u32 t[8] = {0xdd8b6d21u, 0x352ff640u, 0x331ce10au, 0x011e8bd1u,
+                                 0x55d392c2u, 0x438150aeu, 0x73335b20u, 0x21fe9388u};
+        return t[i];
+    }
     // 2^256 - m and -m^-1 mod 2^256 (the constants of the Shoup product by a fixed factor)
     ZK_DI static constexpr u32 np(int i) {
         constexpr u32 t[8] = {0x0fffffffu, 0xbc1e0a6cu, 0x86468f6eu, 0xd7cc17b7u,
@@ -94,6 +100,11 @@ struct FqParams {
         return t[i];
     }
     static constexpr u32 MPRIME = 3834012553u;
+    ZK_DI static constexpr u32 invk(int i) {
+        constexpr u32 t[8] = {0x13bd45e1u, 0x31d6a0d9u, 0x382c59a2u, 0x45fbf2bcu,
+                                 0x1ab31dfbu, 0x5b5fa369u, 0xb36fd339u, 0x24811383u};
+        return t[i];
+    }
 };
 
 template <class P>
