@@ -21,15 +21,20 @@
 namespace zk {
 namespace poly {
 
-constexpr u32 CHUNK = 64;   // elements folded by one thread on the first level
+constexpr u32 CHUNK = 64;   // elements folded by one evaluation thread on the first level
+// the same for the product scans, inversion and division, whose threads run one dependent
+// chain each (evaluation runs four): 32 gives them twice the chains of 64 (2^22: division
+// 0.365 -> 0.324 ms, inversion 0.487 -> 0.435 ms, product scan 0.332 -> 0.294 ms; 16 is no
+// faster at 2^22 and slower at 2^24)
+constexpr u32 SWEEP = 32;
 constexpr u32 UPPER = 8;    // on the upper levels: short chains, since those levels are tiny
 constexpr u32 BLOCK = 128;
 
-// The level sweeps (evaluation, product scans, inversion, division) fold chunks of CHUNK
+// The level sweeps (evaluation, product scans, inversion, division) fold chunks of `first`
 // elements on the input and chunks of UPPER on every level above it: the first level carries
-// the work and wants long chains, the upper levels are a few thousand values whose cost is the
-// length of their dependent chains.
-inline u32 chunk_at(size_t level) { return level == 0 ? CHUNK : UPPER; }
+// the work, the upper levels are a few thousand values whose cost is the length of their
+// dependent chains.
+inline u32 chunk_at(size_t level, u32 first) { return level == 0 ? first : UPPER; }
 
 inline u32 grid_for(u64 items, u32 block, u32 per_sm = 16) {
     const u64 b = (items + block - 1) / block;
@@ -195,10 +200,10 @@ __global__ void __launch_bounds__(BLOCK) scan_down_kernel(View data, u64 n, cons
     }
 }
 
-// top of the inversion tree: one thread inverts the product of at most CHUNK values
+// top of the inversion tree: one thread inverts the product of at most SWEEP values
 __global__ void inv_top_kernel(u32 *vals, u64 m) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    Fr pre[CHUNK];
+    Fr pre[SWEEP];
     Fr acc = Fr::one();
     for (u64 i = 0; i < m; i++) {
         pre[i] = acc;
@@ -213,7 +218,7 @@ __global__ void inv_top_kernel(u32 *vals, u64 m) {
     }
 }
 
-// top of the scan tree: exclusive product scan of at most CHUNK values in place
+// top of the scan tree: exclusive product scan of at most SWEEP values in place
 __global__ void scan_top_kernel(u32 *vals, u64 m) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     Fr acc = Fr::one();
@@ -253,7 +258,7 @@ __global__ void pow_chunk_kernel(const u32 *b, u32 chunk, u32 *out) {
     Fr::pow_u64(Fr::load(b), chunk).canonical().store(out);
 }
 
-// a short level (n <= CHUNK): one thread runs the recurrence directly
+// a short level (n <= SWEEP): one thread runs the recurrence directly
 __global__ void kate_small_kernel(View p, View q, u64 n, const u32 *b) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     const Fr B = Fr::load(b);
@@ -285,11 +290,11 @@ __global__ void __launch_bounds__(BLOCK) kate_down_kernel(View p, View q, u64 n,
 }
 
 // ------------------------------------------------------------------ temp planning
-inline std::vector<u64> level_sizes(u64 n) {
+inline std::vector<u64> level_sizes(u64 n, u32 first) {
     std::vector<u64> s;
     u64 m = n;
-    for (size_t k = 0; m > chunk_at(k); k++) {
-        m = (m + chunk_at(k) - 1) / chunk_at(k);
+    for (size_t k = 0; m > chunk_at(k, first); k++) {
+        m = (m + chunk_at(k, first) - 1) / chunk_at(k, first);
         s.push_back(m);
     }
     return s;  // sizes of the chunk-result arrays; the last one fits in one chunk of its level
@@ -357,7 +362,7 @@ extern "C" cudaError_t scalar_pow(unsigned int *target, unsigned long long exp, 
 extern "C" cudaError_t poly_eval(void *temp_buf, unsigned long *temp_buf_size, ConstPolyPtr poly, unsigned int *res,
                                  const unsigned int *x, cudaStream_t stream) {
     const u64 n = poly.len;
-    std::vector<u64> lv = level_sizes(n);
+    std::vector<u64> lv = level_sizes(n, CHUNK);
     const u32 levels = (u32)lv.size() + 1;
     size_t need = al((size_t)levels * 2 * 32);
     for (u64 m : lv) need += al(m * 32);
@@ -379,7 +384,7 @@ extern "C" cudaError_t poly_eval(void *temp_buf, unsigned long *temp_buf_size, C
     u64 m = n;
     for (u32 k = 0; k < levels; k++) {
         u32 *out = (k + 1 < levels) ? reinterpret_cast<u32 *>(base + off) : res;
-        const u32 chunk = chunk_at(k);
+        const u32 chunk = chunk_at(k, CHUNK);
         const u64 threads = (m + chunk - 1) / chunk;
         const u32 grid = (u32)((threads + BLOCK - 1) / BLOCK);
         if (k == 0)
@@ -400,10 +405,10 @@ extern "C" cudaError_t poly_eval(void *temp_buf, unsigned long *temp_buf_size, C
 extern "C" cudaError_t batched_invert(void *temp_buffer, unsigned long *buffer_size, PolyPtr poly,
                                       cudaStream_t stream) {
     const u64 n = poly.len;
-    std::vector<u64> lv = level_sizes(n);
+    std::vector<u64> lv = level_sizes(n, SWEEP);
     size_t need = al(n * 32);
     for (u64 m : lv) need += 2 * al(m * 32);
-    need += al(CHUNK * 32);
+    need += al(SWEEP * 32);
     if (temp_buffer == nullptr) {
         ZK_CHECK_ARG(buffer_size != nullptr);
         *buffer_size = need;
@@ -434,20 +439,20 @@ extern "C" cudaError_t batched_invert(void *temp_buffer, unsigned long *buffer_s
     const size_t L = data.size();
     for (size_t k = 0; k < L; k++) {
         const u64 m = size[k];
-        const u64 threads = (m + chunk_at(k) - 1) / chunk_at(k);
+        const u64 threads = (m + chunk_at(k, SWEEP) - 1) / chunk_at(k, SWEEP);
         u32 *tot = (k + 1 < L) ? data[k + 1].base : top;
         prod_up_kernel<<<(u32)((threads + BLOCK - 1) / BLOCK), BLOCK, 0, stream>>>(data[k], m, prefix[k], tot, k == 0,
-                                                                                  chunk_at(k));
+                                                                                  chunk_at(k, SWEEP));
         ZK_TRY(cudaGetLastError());
     }
     inv_top_kernel<<<1, 32, 0, stream>>>(top, 1);
     ZK_TRY(cudaGetLastError());
     for (size_t k = L; k-- > 0;) {
         const u64 m = size[k];
-        const u64 threads = (m + chunk_at(k) - 1) / chunk_at(k);
+        const u64 threads = (m + chunk_at(k, SWEEP) - 1) / chunk_at(k, SWEEP);
         const u32 *inv_tot = (k + 1 < L) ? data[k + 1].base : top;
         inv_down_kernel<<<(u32)((threads + BLOCK - 1) / BLOCK), BLOCK, 0, stream>>>(data[k], m, prefix[k], inv_tot,
-                                                                                   chunk_at(k));
+                                                                                   chunk_at(k, SWEEP));
         ZK_TRY(cudaGetLastError());
     }
     return cudaSuccess;
@@ -456,7 +461,7 @@ extern "C" cudaError_t batched_invert(void *temp_buffer, unsigned long *buffer_s
 // ---- scan_mul: inclusive product scan in place; temp = chunk-product arrays
 extern "C" cudaError_t scan_mul(void *temp_buffer, unsigned long *buffer_size, PolyPtr target, cudaStream_t stream) {
     const u64 n = target.len;
-    std::vector<u64> lv = level_sizes(n);
+    std::vector<u64> lv = level_sizes(n, SWEEP);
     size_t need = al(32);
     for (u64 m : lv) need += al(m * 32);
     if (temp_buffer == nullptr) {
@@ -478,17 +483,17 @@ extern "C" cudaError_t scan_mul(void *temp_buffer, unsigned long *buffer_size, P
     }
     const size_t L = data.size();
     for (size_t k = 0; k + 1 < L; k++) {
-        const u64 threads = (size[k] + chunk_at(k) - 1) / chunk_at(k);
+        const u64 threads = (size[k] + chunk_at(k, SWEEP) - 1) / chunk_at(k, SWEEP);
         prod_up_kernel<<<(u32)((threads + BLOCK - 1) / BLOCK), BLOCK, 0, stream>>>(data[k], size[k], nullptr,
                                                                                   data[k + 1].base, false,
-                                                                                  chunk_at(k));
+                                                                                  chunk_at(k, SWEEP));
         ZK_TRY(cudaGetLastError());
     }
     for (size_t k = L; k-- > 0;) {
-        const u64 threads = (size[k] + chunk_at(k) - 1) / chunk_at(k);
+        const u64 threads = (size[k] + chunk_at(k, SWEEP) - 1) / chunk_at(k, SWEEP);
         const u32 *above = (k + 1 < L) ? data[k + 1].base : nullptr;
         scan_down_kernel<<<(u32)((threads + BLOCK - 1) / BLOCK), BLOCK, 0, stream>>>(data[k], size[k], above,
-                                                                                    chunk_at(k));
+                                                                                    chunk_at(k, SWEEP));
         ZK_TRY(cudaGetLastError());
     }
     return cudaSuccess;
@@ -501,7 +506,7 @@ extern "C" cudaError_t scan_mul(void *temp_buffer, unsigned long *buffer_size, P
 extern "C" cudaError_t kate_division(void *temp_buf, unsigned long *temp_buf_size, unsigned int log_p, ConstPolyPtr p,
                                      const unsigned int *b, PolyPtr q, cudaStream_t stream) {
     const u64 n = 1ull << log_p;
-    std::vector<u64> lv = level_sizes(n);
+    std::vector<u64> lv = level_sizes(n, SWEEP);
     size_t need = al((lv.size() + 1) * 32);
     for (u64 m : lv) need += 2 * al(m * 32);
     if (temp_buf == nullptr) {
@@ -525,22 +530,22 @@ extern "C" cudaError_t kate_division(void *temp_buf, unsigned long *temp_buf_siz
         Q.push_back(plain_view(base + off, lv[k]));
         off += al(lv[k] * 32);
         size.push_back(lv[k]);
-        pow_chunk_kernel<<<1, 32, 0, stream>>>(Bs.back(), chunk_at(k), bases + k * 8);
+        pow_chunk_kernel<<<1, 32, 0, stream>>>(Bs.back(), chunk_at(k, SWEEP), bases + k * 8);
         Bs.push_back(bases + k * 8);
     }
     // up-sweeps: P[k+1][t] = chunk-local value of level k at chunk t's start
     for (size_t k = 0; k + 1 < L; k++) {
-        const u64 chunks = (size[k] + chunk_at(k) - 1) / chunk_at(k);
+        const u64 chunks = (size[k] + chunk_at(k, SWEEP) - 1) / chunk_at(k, SWEEP);
         kate_up_kernel<<<(u32)((chunks + BLOCK - 1) / BLOCK), BLOCK, 0, stream>>>(P[k], size[k], Bs[k],
-                                                                                 P[k + 1].base, chunk_at(k));
+                                                                                 P[k + 1].base, chunk_at(k, SWEEP));
         ZK_TRY(cudaGetLastError());
     }
     kate_small_kernel<<<1, 32, 0, stream>>>(P[L - 1], Q[L - 1], size[L - 1], Bs[L - 1]);
     ZK_TRY(cudaGetLastError());
     for (size_t k = L - 1; k-- > 0;) {
-        const u64 chunks = (size[k] + chunk_at(k) - 1) / chunk_at(k);
+        const u64 chunks = (size[k] + chunk_at(k, SWEEP) - 1) / chunk_at(k, SWEEP);
         kate_down_kernel<<<(u32)((chunks + BLOCK - 1) / BLOCK), BLOCK, 0, stream>>>(P[k], Q[k], size[k], Bs[k],
-                                                                                   Q[k + 1].base, chunk_at(k));
+                                                                                   Q[k + 1].base, chunk_at(k, SWEEP));
         ZK_TRY(cudaGetLastError());
     }
     return cudaSuccess;
