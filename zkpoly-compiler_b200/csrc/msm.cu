@@ -90,8 +90,8 @@ ZK_DI u32 find_task(const T *first, u32 ntasks, T x) {
     return lo;
 }
 
-// CTAs per bit class in the bucket reduction (a power of two); the window kernel folds up to
-// 32 classes x 32 parts
+// CTAs per bit class in the bucket reduction (a power of two); scale_kernel and window_kernel
+// fold up to 32 parts and 32 classes, one per lane
 constexpr u32 MAX_PARTS = 32;
 
 inline Task make_task(u64 n, u32 c, u32 n_tables) {
@@ -919,8 +919,8 @@ __global__ void __launch_bounds__(TREE_CTA) tree_down_kernel(u32 *vals, u64 n, c
 // is  sum_g T_g + L * sum_g g U_g,  and  sum_g g U_g = sum_k 2^k X_k  with X_k the sum of the
 // U_g whose index g has bit k set.  segment_kernel forms U_g and T_g (2L additions per
 // thread); class_kernel sums every class (each X_k, and the T_g in two halves) in parallel
-// parts; window_kernel joins the parts, scales X_k by 2^k * L with doublings and adds the
-// classes.  Every chain of dependent additions stays short, so a window of 2^16 buckets is
+// parts; scale_kernel joins each class's parts and scales X_k by 2^k * L with doublings, and
+// window_kernel adds the classes.  Every chain of dependent additions stays short, so a window of 2^16 buckets is
 // reduced by tens of thousands of threads instead of a few thousand long ones.
 __global__ void __launch_bounds__(128) segment_kernel(const Batch b, const u32 *bucket_sums, u32 *seg_u,
                                                      u32 *seg_t) {
@@ -979,41 +979,61 @@ __global__ void __launch_bounds__(256) class_kernel(const Batch b, const u32 *se
     if (threadIdx.x == 0) G1X::load(sm).store(cls_out + (((u64)wg * b.ncls + cls) * b.nparts + part) * 32);
 }
 
-// one CTA (256 threads) per physical window: parts -> classes -> 2^k L X_k -> window value
-__global__ void __launch_bounds__(256) window_kernel(const Batch b, const u32 *cls_out, u32 *win_out) {
-    __shared__ u32 sm[256 * 32];
-    const u32 wg = blockIdx.x;
+// Classes to window values in two launches of single warps, so that the work spreads over as
+// many SMs as there are classes.  scale_kernel, one warp per (window, class): one part per lane
+// (at most 32 parts, a power of two) summed by a shuffle tree of additions; every lane then
+// holds the class sum X_k and the warp scales it by 2^k L with warp-wide doublings (each
+// doubling's independent products side by side, g1_dbl_warp), the longest dependent chain of
+// the reduction (up to 18 doublings); the result replaces part 0 of the class.  window_kernel,
+// one warp per window: one class per lane (at most 32), summed by a shuffle tree.
+ZK_DI G1X g1x_shfl_down(const G1X &p, u32 d) {
+    G1X r;
+#pragma unroll
+    for (int w = 0; w < 8; w++) {
+        r.x.v[w] = __shfl_down_sync(0xffffffffu, p.x.v[w], d);
+        r.y.v[w] = __shfl_down_sync(0xffffffffu, p.y.v[w], d);
+        r.zz.v[w] = __shfl_down_sync(0xffffffffu, p.zz.v[w], d);
+        r.zzz.v[w] = __shfl_down_sync(0xffffffffu, p.zzz.v[w], d);
+    }
+    return r;
+}
+ZK_DI G1X g1x_bcast(const G1X &p, int src) {
+    G1X r;
+    r.x = lane_bcast(p.x, src);
+    r.y = lane_bcast(p.y, src);
+    r.zz = lane_bcast(p.zz, src);
+    r.zzz = lane_bcast(p.zzz, src);
+    return r;
+}
+
+// grid (windows, classes), 32 threads
+__global__ void __launch_bounds__(32) scale_kernel(const Batch b, u32 *cls_out) {
+    const u32 wg = blockIdx.x, cl = blockIdx.y, lane = threadIdx.x;
     const u32 t = find_task(b.win_first, b.ntasks, wg);
     const Task &k = b.task[t];
-    const u32 ncls = k.gbits + 2, P = k.parts, tid = threadIdx.x;
-    // thread (class tid / 8, lane tid % 8) first sums the parts p = lane, lane + 8, ...; then a
-    // tree over the 8 lanes of each class
-    const u32 cl = tid >> 3, sub = tid & 7;
-    G1X v = G1X::identity();
-    if (cl < ncls)
-        for (u32 p = sub; p < P; p += 8)
-            v = g1_add(v, G1X::load(cls_out + (((u64)wg * b.ncls + cl) * b.nparts + p) * 32));
-    v.store(sm + tid * 32);
-    __syncthreads();
-    for (u32 st = 4; st > 0; st >>= 1) {
-        if (cl < ncls && sub < st) {
-            G1X x = G1X::load(sm + tid * 32);
-            G1X y = G1X::load(sm + (tid + st) * 32);
-            g1_add(x, y).store(sm + tid * 32);
-        }
-        __syncthreads();
+    if (cl >= k.gbits + 2) return;  // the whole warp leaves together
+    const u32 P = k.parts;
+    u32 *base = cls_out + ((u64)wg * b.ncls + cl) * b.nparts * 32;
+    G1X v = lane < P ? G1X::load(base + (u64)lane * 32) : G1X::identity();
+    for (u32 d = P >> 1; d > 0; d >>= 1) v = g1_add(v, g1x_shfl_down(v, d));
+    if (cl < k.gbits) {
+        v = g1x_bcast(v, 0);
+        const u32 dbls = cl + (31 - __clz(k.L));  // 2^cl * L
+        for (u32 i = 0; i < dbls; i++) v = g1_dbl_warp(v);
     }
-    G1X x = G1X::identity();
-    if (tid < ncls) {
-        x = G1X::load(sm + tid * 8 * 32);
-        if (tid < k.gbits) {
-            const u32 dbls = tid + (31 - __clz(k.L));  // 2^tid * L
-            for (u32 i = 0; i < dbls; i++) x = g1_dbl(x);
-        }
-    }
-    __syncthreads();
-    cta_tree_sum(sm, x);
-    if (tid == 0) G1X::load(sm).store(win_out + (u64)wg * 32);
+    if (lane == 0) v.store(base);
+}
+
+// one warp per physical window: the sum of its classes' scaled values
+__global__ void __launch_bounds__(32) window_kernel(const Batch b, const u32 *cls_out, u32 *win_out) {
+    const u32 wg = blockIdx.x, lane = threadIdx.x;
+    const u32 t = find_task(b.win_first, b.ntasks, wg);
+    const Task &k = b.task[t];
+    const u32 ncls = k.gbits + 2;
+    G1X v = lane < ncls ? G1X::load(cls_out + ((u64)wg * b.ncls + lane) * b.nparts * 32) : G1X::identity();
+    const u32 span = 1u << (32 - __clz(ncls - 1));  // ncls >= 2 rounded up to a power of two
+    for (u32 d = span >> 1; d > 0; d >>= 1) v = g1_add(v, g1x_shfl_down(v, d));
+    if (lane == 0) v.store(win_out + (u64)wg * 32);
 }
 
 // ------------------------------------------------------------------ 6: window combination
@@ -1220,7 +1240,9 @@ cudaError_t run_batch(const Batch &b, const Layout &l, char *ws, cudaStream_t st
         class_kernel<<<dim3((u32)l.wins, b.ncls, b.nparts), 256, 0, stream>>>(b, seg, seg + l.segs * 32, cls);
         ZK_TRY(cudaGetLastError());
         prof.mark("classes", stream);
-        window_kernel<<<(u32)l.wins, 256, 0, stream>>>(b, cls, win);
+        scale_kernel<<<dim3((u32)l.wins, b.ncls), 32, 0, stream>>>(b, cls);
+        ZK_TRY(cudaGetLastError());
+        window_kernel<<<(u32)l.wins, 32, 0, stream>>>(b, cls, win);
         ZK_TRY(cudaGetLastError());
     }
     prof.mark("window_sum", stream);
